@@ -1,0 +1,501 @@
+// capi.cpp -- the C ABI (include/gmapf_c.h): lifecycle rules and host-side
+// bookkeeping of gmapf::GMAPF (src/GMAPF.cu), with the reference's
+// exceptions turned into status codes and a per-thread error message.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "internal.h"
+
+using namespace gmapf_b200;
+
+struct gmapf_ctx {
+    Context c;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+gmapf_status fail(int code, const std::string& msg) {
+    g_err = msg;
+    return (gmapf_status)code;
+}
+
+#define NEED_CTX(ctx) \
+    if (!(ctx)) return fail(GMAPF_E_INVALID_ARG, "null context")
+
+// PathFinder threads per agent: the reference packs 128/T requests per block
+// (PathFinder.h:559-572) and seeds lanes 0 and 1 (PathFinder.h:168-189).
+bool valid_T(int t) { return t == 2 || t == 4 || t == 8 || t == 16 || t == 32; }
+
+int locate_host(const Context& c, float x, float y) {
+    LocateGrid g = c.map.view();
+    return locate(g, x, y);
+}
+
+std::string v2s(float x, float y) {
+    char b[96];
+    std::snprintf(b, sizeof(b), "(%f, %f)", x, y);
+    return b;
+}
+
+int add_dirty(Context& c, int id, int node, float x, float y) {
+    int4 r;
+    r.x = id;
+    r.y = node;
+    std::memcpy(&r.z, &x, 4);
+    std::memcpy(&r.w, &y, 4);
+    int& slot = c.dirty_slot[id];
+    if (slot >= 0)
+        c.dirty_recs[slot] = r;
+    else {
+        slot = (int)c.dirty_recs.size();
+        c.dirty_recs.push_back(r);
+    }
+    return GMAPF_OK;
+}
+
+gmapf_status start_if_needed(Context& c) {
+    if (c.started) return GMAPF_OK;
+    if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
+    std::string err;
+    int rc = device_start(c, err);
+    if (rc) {
+        device_free(c);
+        return fail(rc, err);
+    }
+    c.started = true;
+    if (c.opt.autotune) {
+        rc = device_autotune(c, err);
+        if (rc) return fail(rc, err);
+    }
+    return GMAPF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gmapf_last_error(void) { return g_err.c_str(); }
+
+gmapf_status gmapf_create(gmapf_ctx** out) {
+    if (!out) return fail(GMAPF_E_INVALID_ARG, "null output pointer");
+    *out = new (std::nothrow) gmapf_ctx();
+    if (!*out) return fail(GMAPF_E_CAPACITY, "out of host memory");
+    (*out)->c.opt.device = 0;
+    (*out)->c.opt.mode = GMAPF_MODE_BATCHED;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_destroy(gmapf_ctx* ctx) {
+    if (!ctx) return GMAPF_OK;
+    Context& c = ctx->c;
+    if (c.started) {
+        if (c.step_going) {
+            std::string err;
+            device_wait_step(c, err);
+            c.step_going = false;
+        }
+        device_free(c);
+    }
+    delete ctx;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_init(gmapf_ctx* ctx, const gmapf_config* cfg) {
+    NEED_CTX(ctx);
+    if (!cfg) return fail(GMAPF_E_INVALID_ARG, "null config");
+    Context& c = ctx->c;
+    if (c.inited) return fail(GMAPF_E_STATE, "already initialized");
+    if (cfg->AgentsMaxCount < 0) return fail(GMAPF_E_INVALID_ARG, "AgentsMaxCount must be >= 0");
+    if (!valid_T(cfg->PathFinderThreadsPerAgents))
+        return fail(GMAPF_E_INVALID_ARG, "PathFinderThreadsPerAgents must be one of 2, 4, 8, 16, 32");
+    // the per-lane queues live in shared memory (12 bytes per entry per thread)
+    if (cfg->PathFinderQueueCapacity < 1 || cfg->PathFinderQueueCapacity > 512)
+        return fail(GMAPF_E_INVALID_ARG, "PathFinderQueueCapacity must be in [1, 512]");
+    if (cfg->PathFinderParallelAgents < 0) return fail(GMAPF_E_INVALID_ARG, "PathFinderParallelAgents must be >= 0");
+    c.cfg = *cfg;
+    c.T = cfg->PathFinderThreadsPerAgents;
+    c.C = cfg->PathFinderQueueCapacity;
+    c.K = cfg->PathFinderHeuristicK;
+    c.block_threads = 128;
+    const int cap = cfg->AgentsMaxCount;
+    c.m_pos.reserve(cap);
+    c.m_state.reserve(cap);
+    c.m_cur.reserve(cap);
+    c.m_targ.reserve(cap);
+    c.m_targ_node.reserve(cap);
+    c.dirty_slot.reserve(cap);
+    c.inited = true;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_set_options(gmapf_ctx* ctx, const gmapf_options* o) {
+    NEED_CTX(ctx);
+    if (!o) return fail(GMAPF_E_INVALID_ARG, "null options");
+    Context& c = ctx->c;
+    if (c.started) return fail(GMAPF_E_STATE, "options must be set before start");
+    if (o->mode != GMAPF_MODE_BATCHED && o->mode != GMAPF_MODE_PLAIN)
+        return fail(GMAPF_E_INVALID_ARG, "unknown mode");
+    if (o->block_threads != 0 &&
+        (o->block_threads < 32 || o->block_threads > 256 || o->block_threads % 32 != 0))
+        return fail(GMAPF_E_INVALID_ARG, "block_threads must be 0 or a multiple of 32 in [32, 256]");
+    if (o->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
+    c.opt = *o;
+    if (o->block_threads) c.block_threads = o->block_threads;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_get_options(gmapf_ctx* ctx, gmapf_options* out) {
+    NEED_CTX(ctx);
+    if (!out) return fail(GMAPF_E_INVALID_ARG, "null output");
+    *out = ctx->c.opt;
+    out->block_threads = ctx->c.block_threads;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_fill_map_start(gmapf_ctx* ctx, float sx, float sy) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:133-145
+    c.cdt_v = {0.f, 0.f, 0.f, sy, sx, sy, sx, 0.f};
+    c.cdt_e = {0, 1, 1, 2, 2, 3, 3, 0};
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_fill_map_obstacle(gmapf_ctx* ctx, const gmapf_v2* v, int32_t count) {
+    NEED_CTX(ctx);
+    if (count > 0 && !v) return fail(GMAPF_E_INVALID_ARG, "null vertices");
+    if (count <= 0) return fail(GMAPF_E_INVALID_ARG, "an obstacle needs at least one vertex");
+    Context& c = ctx->c;
+    // src/GMAPF.cu:147-159: a closed polygon
+    const unsigned start = (unsigned)(c.cdt_v.size() / 2);
+    for (int i = 0; i < count; i++) {
+        const unsigned idx = (unsigned)(c.cdt_v.size() / 2);
+        c.cdt_v.push_back(v[i].X);
+        c.cdt_v.push_back(v[i].Y);
+        if (i > 0) {
+            c.cdt_e.push_back(idx - 1);
+            c.cdt_e.push_back(idx);
+        }
+    }
+    c.cdt_e.push_back((unsigned)(c.cdt_v.size() / 2 - 1));
+    c.cdt_e.push_back(start);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_fill_map_manually(gmapf_ctx* ctx, const gmapf_node* nodes, int32_t count);
+
+gmapf_status gmapf_fill_map_end(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.started) return fail(GMAPF_E_STATE, "cannot modify map after start");
+    if (c.map_filled) return fail(GMAPF_E_STATE, "map is already filled");
+    std::vector<gmapf_node> nodes;
+    std::string err;
+    int rc = build_navmesh_cdt(c.cdt_v, c.cdt_e, nodes, err);
+    if (rc) return fail(rc, err);
+    return gmapf_fill_map_manually(ctx, nodes.data(), (int32_t)nodes.size());
+}
+
+gmapf_status gmapf_fill_map_manually(gmapf_ctx* ctx, const gmapf_node* nodes, int32_t count) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:199-217
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.started) return fail(GMAPF_E_STATE, "cannot modify map after start");
+    if (c.map_filled) return fail(GMAPF_E_STATE, "map is already filled");
+    if (count < 0 || (count > 0 && !nodes)) return fail(GMAPF_E_INVALID_ARG, "bad node array");
+    for (int i = 0; i < count; i++)
+        for (int k = 0; k < 3; k++) {
+            const int nb = nodes[i].NeibsIdx[k];
+            if (nb < -1 || nb >= count)
+                return fail(GMAPF_E_INVALID_ARG, "node " + std::to_string(i) + " has neighbour " +
+                                                     std::to_string(nb) + " outside the map");
+        }
+    build_host_map(nodes, count, c.map);
+    c.map_filled = true;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:219-236
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.started) return fail(GMAPF_E_STATE, "cannot add agents after start");
+    if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
+    if (c.A >= c.cfg.AgentsMaxCount) return fail(GMAPF_E_CAPACITY, "AgentsMaxCount reached");
+    const int node = locate_host(c, x, y);
+    if (node < 0) return fail(GMAPF_E_INVALID_POS, "initial pos " + v2s(x, y) + " is invalid");
+    c.m_pos.push_back(gmapf_v2{x, y});
+    c.m_state.push_back(GMAPF_AGENT_IDLE);
+    c.m_cur.push_back(node);
+    c.m_targ.push_back(gmapf_v2{0.f, 0.f});
+    c.m_targ_node.push_back(-1);
+    c.dirty_slot.push_back(-1);
+    if (out_id) *out_id = c.A;
+    c.A++;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t id, float x, float y) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:238-253
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
+    if (id < 0 || id >= c.A) return fail(GMAPF_E_INVALID_ARG, "agent id " + std::to_string(id) + " out of range");
+    const int node = locate_host(c, x, y);
+    if (node < 0) return fail(GMAPF_E_INVALID_POS, "target pos " + v2s(x, y) + " is invalid");
+    c.m_state[id] = GMAPF_AGENT_SEARCH;
+    c.m_targ[id] = gmapf_v2{x, y};
+    c.m_targ_node[id] = node;
+    if (c.started) add_dirty(c, id, node, x, y);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* pos, int32_t n) {
+    NEED_CTX(ctx);
+    if (n < 0 || (n > 0 && (!ids || !pos))) return fail(GMAPF_E_INVALID_ARG, "bad bulk arrays");
+    for (int k = 0; k < n; k++) {
+        gmapf_status s = gmapf_set_agent_targ_pos(ctx, ids[k], pos[k].X, pos[k].Y);
+        if (s != GMAPF_OK) return s;
+    }
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_manual_start(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:72-130
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.started) return fail(GMAPF_E_STATE, "already started");
+    return start_if_needed(c);
+}
+
+gmapf_status gmapf_async_step(gmapf_ctx* ctx, float dt) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:255-289
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.step_going) return GMAPF_OK;
+    gmapf_status s = start_if_needed(c);
+    if (s != GMAPF_OK) return s;
+    std::string err;
+    int rc = device_async_step(c, dt, err);
+    if (rc) return fail(rc, err);
+    c.step_going = true;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_wait_step_end(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:291-314
+    if (!c.step_going) return GMAPF_OK;
+    std::string err;
+    int rc = device_wait_step(c, err);
+    c.step_going = false;
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_get_agent_pos(gmapf_ctx* ctx, int32_t id, gmapf_v2* out) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (id < 0 || id >= c.A || !out) return fail(GMAPF_E_INVALID_ARG, "agent id out of range");
+    *out = c.m_pos[id];
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_get_agent_state(gmapf_ctx* ctx, int32_t id, int32_t* out) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (id < 0 || id >= c.A || !out) return fail(GMAPF_E_INVALID_ARG, "agent id out of range");
+    *out = c.m_state[id];
+    return GMAPF_OK;
+}
+
+const gmapf_v2* gmapf_agent_pos_view(gmapf_ctx* ctx) { return ctx ? ctx->c.m_pos.data() : nullptr; }
+
+gmapf_status gmapf_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* state, int32_t n) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (n < 0 || n > c.A) return fail(GMAPF_E_INVALID_ARG, "n out of range");
+    if (pos) std::memcpy(pos, c.m_pos.data(), sizeof(gmapf_v2) * n);
+    if (state) std::memcpy(state, c.m_state.data(), sizeof(int32_t) * n);
+    return GMAPF_OK;
+}
+
+int32_t gmapf_agent_count(gmapf_ctx* ctx) { return ctx ? ctx->c.A : 0; }
+
+gmapf_status gmapf_profiler_dump(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    // src/GMAPF.cu:326-356, same line format
+    if (!c.cfg.IsProfiler) return fail(GMAPF_E_STATE, "profiler disabled");
+    const Profiler& p = c.prof;
+    auto line = [](const char* t, float sum, float mx, int n) {
+        std::printf("%s avg: %g max: %g\n", t, n > 0 ? sum / n : 0.0f, mx);
+    };
+    std::printf("[gmapf]----------------------\n");
+    line("[gmapf] step", p.sum_wall, p.max_wall, p.n);
+    line("[gmapf] ---step post copy", p.sum_post, p.max_post, p.n);
+    std::printf("\n[gmapf] path finder\n");
+    line("[gmapf] find requests", p.sum_compact, p.max_compact, p.n);
+    line("[gmapf] search", p.sum_search, p.max_search, p.n_search);
+    std::printf("\n[gmapf] agents mover\n");
+    line("[gmapf] move+collisions+progress", p.sum_mover, p.max_mover, p.n_mover);
+    std::printf("[gmapf]----------------------\n");
+    std::fflush(stdout);
+    return GMAPF_OK;
+}
+
+int32_t gmapf_map_count(gmapf_ctx* ctx) { return ctx ? ctx->c.map.n : 0; }
+
+gmapf_status gmapf_get_map_nodes(gmapf_ctx* ctx, gmapf_node* out, int32_t cap) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
+    if (!out || cap < c.map.n) return fail(GMAPF_E_INVALID_ARG, "output too small");
+    std::memcpy(out, c.map.nodes.data(), sizeof(gmapf_node) * c.map.n);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_locate_points(gmapf_ctx* ctx, const gmapf_v2* pts, int32_t n, int32_t* out) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
+    if (n < 0 || (n > 0 && (!pts || !out))) return fail(GMAPF_E_INVALID_ARG, "bad arrays");
+    LocateGrid g = c.map.view();
+    for (int i = 0; i < n; i++) out[i] = locate(g, pts[i].X, pts[i].Y);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_debug_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* state, int32_t* cur,
+                                    int32_t* targ, int32_t* step_idx, int32_t* step_node,
+                                    gmapf_v2* step_pos, int32_t* path_len) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.started) return fail(GMAPF_E_STATE, "not started");
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    std::string err;
+    int rc = device_debug_agents(c, pos, state, cur, targ, step_idx, step_node, step_pos, path_len, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_debug_get_path(gmapf_ctx* ctx, int32_t id, int32_t* out, int32_t cap, int32_t* out_len) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.started) return fail(GMAPF_E_STATE, "not started");
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    if (id < 0 || id >= c.A || !out_len || (cap > 0 && !out)) return fail(GMAPF_E_INVALID_ARG, "bad arguments");
+    std::string err;
+    int rc = device_debug_path(c, id, out, cap, out_len, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_last_step_stats(gmapf_ctx* ctx, gmapf_step_stats* out) {
+    NEED_CTX(ctx);
+    if (!out) return fail(GMAPF_E_INVALID_ARG, "null output");
+    *out = ctx->c.last;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_step_time_percentile(gmapf_ctx* ctx, float q, float* out_ms) {
+    NEED_CTX(ctx);
+    if (!out_ms || q < 0 || q > 100) return fail(GMAPF_E_INVALID_ARG, "bad arguments");
+    std::vector<float> v = ctx->c.prof.wall_ms;
+    if (v.empty()) {
+        *out_ms = 0;
+        return GMAPF_OK;
+    }
+    std::sort(v.begin(), v.end());
+    // nearest-rank percentile
+    size_t k = (size_t)std::ceil(q / 100.0 * v.size());
+    if (k > 0) k--;
+    if (k >= v.size()) k = v.size() - 1;
+    *out_ms = v[k];
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_reset_profiler(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    ctx->c.prof = Profiler{};
+    return GMAPF_OK;
+}
+
+int64_t gmapf_kernel_launches(gmapf_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+
+gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, const int32_t* d_targets,
+                                       int32_t n, int32_t* d_found, int32_t* d_lens, int32_t* d_paths,
+                                       int32_t path_stride, gmapf_step_stats* stats) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    if (n < 0 || path_stride < 1) return fail(GMAPF_E_INVALID_ARG, "bad sizes");
+    if (n > 0 && (!d_starts || !d_targets || !d_found || !d_lens || !d_paths))
+        return fail(GMAPF_E_INVALID_ARG, "null device pointer");
+    gmapf_status s = start_if_needed(c);
+    if (s != GMAPF_OK) return s;
+    std::string err;
+    int rc = device_search_batch(c, d_starts, d_targets, n, d_found, d_lens, d_paths, path_stride, stats, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_search_batch_host(gmapf_ctx* ctx, const int32_t* starts, const int32_t* targets,
+                                     int32_t n, int32_t* found, int32_t* lens, int32_t* paths,
+                                     int32_t path_stride, gmapf_step_stats* stats) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    if (n < 0 || path_stride < 1) return fail(GMAPF_E_INVALID_ARG, "bad sizes");
+    if (n > 0 && (!starts || !targets || !found || !lens || !paths))
+        return fail(GMAPF_E_INVALID_ARG, "null host pointer");
+    for (int i = 0; i < n; i++)
+        if (starts[i] < 0 || starts[i] >= c.map.n || targets[i] < 0 || targets[i] >= c.map.n)
+            return fail(GMAPF_E_INVALID_ARG, "query " + std::to_string(i) + " names a node outside the map");
+    gmapf_status s = start_if_needed(c);
+    if (s != GMAPF_OK) return s;
+    std::string err;
+    int rc = device_upload_batch_io(c, n, path_stride, err);
+    if (rc) return fail(rc, err);
+    Device& d = c.dev;
+    cudaStream_t st = d.stream;
+    cudaError_t e = cudaSuccess;
+    if (n > 0) {
+        e = cudaMemcpyAsync(d.bstarts, starts, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d.btargets, targets, sizeof(int) * n, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return fail(GMAPF_E_CUDA, std::string("upload failed: ") + cudaGetErrorString(e));
+    }
+    rc = device_search_batch(c, d.bstarts, d.btargets, n, d.bfound, d.blens, d.bpaths, path_stride, stats, err);
+    if (rc) return fail(rc, err);
+    if (n > 0) {
+        e = cudaMemcpyAsync(found, d.bfound, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(lens, d.blens, sizeof(int) * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(paths, d.bpaths, sizeof(int) * (size_t)n * path_stride, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(GMAPF_E_CUDA, std::string("download failed: ") + cudaGetErrorString(e));
+    }
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_last_search_ms(gmapf_ctx* ctx, float* out_ms) {
+    NEED_CTX(ctx);
+    if (!out_ms) return fail(GMAPF_E_INVALID_ARG, "null output");
+    *out_ms = ctx->c.last_search_ms;
+    return GMAPF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,684 @@
+// device.cu -- device state and per-frame orchestration.
+//
+// Reference orchestration: src/GMAPF.cu:72-130 (ManualStart), :255-289
+// (AsyncStep), :291-314 (WaitStepEnd); PathFinder.h:354-409 / AgentsMover.h
+// :211-252 (module init); PathFinder.h:508-598 / AgentsMover.h:345-424 (phase
+// launches).  The reference reads the request and mover counts back to the
+// host in the middle of every frame and copies the whole 64-byte-per-agent
+// array both ways synchronously.  Here:
+//   - agents live on the device as structure-of-arrays; SetAgentTargPos
+//     uploads only the changed agents (16 bytes each) before the frame;
+//   - batched form: the frame (compaction, persistent search on one stream,
+//     mover on a second stream, D2H of positions and states) is one CUDA
+//     graph; counts stay on the device;
+//   - plain form: the same kernels launched one by one with the reference's
+//     host read-back of the counts and one static search launch per chunk
+//     of requests.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+
+namespace gmapf_b200 {
+
+#define CK(x)                                                                        \
+    do {                                                                             \
+        cudaError_t e_ = (x);                                                        \
+        if (e_ != cudaSuccess) {                                                     \
+            err = std::string(#x) + " failed: " + cudaGetErrorString(e_);            \
+            return GMAPF_E_CUDA;                                                     \
+        }                                                                            \
+    } while (0)
+
+namespace {
+
+enum Counter { CT_REQ = 0, CT_MOVE = 1, CT_WORK = 2, CT_ERR = 3, CT_COUNT = 16 };
+
+template <class T>
+int dalloc(Context& c, T** p, size_t count, std::string& err) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) {
+        err = std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e);
+        cudaGetLastError();
+        *p = nullptr;
+        return e == cudaErrorMemoryAllocation ? GMAPF_E_CAPACITY : GMAPF_E_CUDA;
+    }
+    c.dev.allocs.push_back((void*)*p);
+    e = cudaMemset(*p, 0, bytes);
+    if (e != cudaSuccess) {
+        err = std::string("cudaMemset failed: ") + cudaGetErrorString(e);
+        return GMAPF_E_CUDA;
+    }
+    return GMAPF_OK;
+}
+
+#define DALLOC(ptr, count)                                \
+    do {                                                  \
+        int rc_ = dalloc(c, &(ptr), (count), err);        \
+        if (rc_ != GMAPF_OK) return rc_;                  \
+    } while (0)
+
+SearchParams search_params(Context& c) {
+    Device& d = c.dev;
+    SearchParams p{};
+    p.rows = d.rows;
+    p.cen = d.cen;
+    p.n = c.map.n;
+    p.req = d.req;
+    p.req_count_d = d.counters + CT_REQ;
+    p.req_count_h = 0;
+    p.T = c.T;
+    p.C = c.C;
+    p.K = c.K;
+    p.rec = d.rec;
+    p.epoch = d.epoch;
+    p.slots = d.slots;
+    p.work_ctr = d.counters + CT_WORK;
+    p.max_rounds = 4 * c.map.n + 64;
+    p.paths = d.paths;
+    p.path_stride = d.path_stride;
+    p.ag_state = d.state;
+    p.ag_step_idx = d.step_idx;
+    p.ag_path_len = d.path_len;
+    p.stats = d.stats;
+    p.err = d.counters + CT_ERR;
+    return p;
+}
+
+MoverParams mover_params(Context& c) {
+    Device& d = c.dev;
+    MoverParams p{};
+    p.A = c.A;
+    p.mv_count = d.counters + CT_MOVE;
+    p.in_move = d.in_move;
+    p.pos = d.pos;
+    p.pos_mid = d.pos_mid;
+    p.step_pos = d.step_pos;
+    p.targ_pos = d.targ_pos;
+    p.state = d.state;
+    p.cur_node = d.cur;
+    p.step_idx = d.step_idx;
+    p.step_node = d.step_node;
+    p.path_len = d.path_len;
+    p.paths = d.paths;
+    p.path_stride = d.path_stride;
+    p.step = reinterpret_cast<const float*>(d.counters + 8);
+    p.cd = c.cfg.AgentRadius * 2.5f;  // AgentsMover.h:222
+    p.cd2 = p.cd * p.cd;
+    p.arrive = FLT_EPSILON + c.cfg.AgentRadius;  // AgentsMover.h:162,224
+    // V2Float::GetRotated(10): cos/sin of 10 degrees, taken in double, rounded to float
+    const double ang = 10.0 * 3.14159265358979323846 / 180.0;
+    p.cs = (float)std::cos(ang);
+    p.sn = (float)std::sin(ang);
+    const HostMap& m = c.map;
+    double w = std::max(1e-3, (double)m.bx1 - m.bx0), h = std::max(1e-3, (double)m.by1 - m.by0);
+    double cell = std::max((double)p.cd * 1.0625, 1e-4);
+    cell = std::max(cell, std::sqrt(w * h / std::max(1.0, 4.0 * c.A)));
+    cell = std::max(cell, std::max(w, h) / 2048.0);
+    p.ax0 = m.bx0;
+    p.ay0 = m.by0;
+    p.ainv = (float)(1.0 / cell);
+    p.aw = std::max(1, (int)std::ceil(w / cell) + 1);
+    p.ah = std::max(1, (int)std::ceil(h / cell) + 1);
+    p.cell_of = d.cell_of;
+    p.cell_cnt = d.cell_cnt;
+    p.cell_start = d.cell_start;
+    p.cell_fill = d.cell_fill;
+    p.cell_items = d.cell_items;
+    p.loc.x0 = m.gx0;
+    p.loc.y0 = m.gy0;
+    p.loc.inv = m.ginv;
+    p.loc.w = m.gw;
+    p.loc.h = m.gh;
+    p.loc.start = d.gstart;
+    p.loc.list = d.glist;
+    p.loc.degen = d.degen;
+    p.loc.ndegen = (int)m.degen.size();
+    p.loc.tri = d.tri;
+    p.loc.n = m.n;
+    p.cen = d.cen;
+    p.n = m.n;
+    p.stats = d.stats;
+    p.err = d.counters + CT_ERR;
+    return p;
+}
+
+int pick_slots(Context& c, int& blocks, std::string& err) {
+    Device& d = c.dev;
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device));
+    if (c.opt.block_threads == 0) {
+        // largest block (up to 128 threads) whose queues fit in shared memory
+        for (int cand : {128, 64, 32}) {
+            if (cand % c.T) continue;
+            c.block_threads = cand;
+            if (search_max_blocks_per_sm(c.T, c.C, cand) > 0) break;
+        }
+    }
+    const int bt = c.block_threads;
+    int per_sm = search_max_blocks_per_sm(c.T, c.C, bt);
+    if (per_sm <= 0) {
+        err = "search kernel cannot be resident with T=" + std::to_string(c.T) +
+              " C=" + std::to_string(c.C) + " block=" + std::to_string(bt);
+        return GMAPF_E_INVALID_ARG;
+    }
+    const int gpb = bt / c.T;
+    long long occ_slots = (long long)sms * per_sm * gpb;
+    size_t freeb = 0, totalb = 0;
+    CK(cudaMemGetInfo(&freeb, &totalb));
+    long long budget = c.opt.search_mem_budget > 0 ? c.opt.search_mem_budget : (40ll << 30);
+    budget = std::min<long long>(budget, (long long)(freeb * 0.6));
+    const long long per_slot = (long long)std::max(1, c.map.n) * (long long)sizeof(Rec);
+    long long mem_slots = budget / per_slot;
+    long long slots = std::min(occ_slots, mem_slots);
+    slots = (slots / gpb) * gpb;
+    if (slots < gpb) {
+        err = "not enough device memory for one block of search slots";
+        return GMAPF_E_CAPACITY;
+    }
+    blocks = (int)(slots / gpb);
+    d.slots = (int)slots;
+    return GMAPF_OK;
+}
+
+int alloc_search_state(Context& c, std::string& err) {
+    Device& d = c.dev;
+    int blocks = 0;
+    int rc = pick_slots(c, blocks, err);
+    if (rc) return rc;
+    DALLOC(d.rec, (size_t)d.slots * std::max(1, c.map.n));
+    DALLOC(d.epoch, (size_t)d.slots);
+    return GMAPF_OK;
+}
+
+void free_search_state(Context& c) {
+    Device& d = c.dev;
+    for (void*& p : d.allocs) {
+        if (p == (void*)d.rec || p == (void*)d.epoch) {
+            cudaFree(p);
+            p = nullptr;
+        }
+    }
+    d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), nullptr), d.allocs.end());
+    d.rec = nullptr;
+    d.epoch = nullptr;
+    d.slots = 0;
+}
+
+int search_blocks(Context& c) { return c.dev.slots / (c.block_threads / c.T); }
+
+void destroy_graph(Context& c) {
+    if (c.dev.graph_exec) cudaGraphExecDestroy(c.dev.graph_exec);
+    if (c.dev.graph) cudaGraphDestroy(c.dev.graph);
+    c.dev.graph_exec = nullptr;
+    c.dev.graph = nullptr;
+}
+
+// kernels of one frame on the two streams (batched form: captured)
+int enqueue_frame(Context& c, bool timing, std::string& err) {
+    Device& d = c.dev;
+    cudaStream_t s = d.stream, s2 = d.stream2;
+    if (timing) CK(cudaEventRecordWithFlags(d.ev[0], s, cudaEventRecordExternal));
+    CK(cudaMemsetAsync(d.counters + CT_ERR, 0, sizeof(int), s));
+    launch_compact(s, c.A, d.state, d.cur, d.targ, c.cfg.PathFinderParallelAgents, d.req,
+                   d.counters + CT_REQ, d.in_move, d.counters + CT_MOVE, d.counters + CT_WORK, d.stats);
+    if (timing) CK(cudaEventRecordWithFlags(d.ev[1], s, cudaEventRecordExternal));
+    CK(cudaEventRecord(d.ev[5], s));
+    CK(cudaStreamWaitEvent(s2, d.ev[5], 0));
+    // search branch
+    SearchParams sp = search_params(c);
+    CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0));
+    if (timing) CK(cudaEventRecordWithFlags(d.ev[2], s, cudaEventRecordExternal));
+    // mover branch
+    MoverParams mp = mover_params(c);
+    if (c.A > 0) {
+        CK(cudaMemsetAsync(d.cell_cnt, 0, sizeof(int) * (d.cells + 1), s2));
+        launch_move_bin(s2, mp);
+        launch_cell_scan(s2, mp);
+        launch_scatter(s2, mp);
+        launch_collide_progress(s2, mp);
+    }
+    if (timing) CK(cudaEventRecordWithFlags(d.ev[3], s2, cudaEventRecordExternal));
+    CK(cudaEventRecord(d.ev[6], s2));
+    CK(cudaStreamWaitEvent(s, d.ev[6], 0));
+    if (c.A > 0) {
+        CK(cudaMemcpyAsync(c.h_pos_stage, d.pos, sizeof(float2) * c.A, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(c.h_state_stage, d.state, sizeof(int) * c.A, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaMemcpyAsync(c.h_small, d.counters, sizeof(int) * CT_COUNT, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(c.h_stats, d.stats, sizeof(unsigned long long) * ST_COUNT, cudaMemcpyDeviceToHost, s));
+    if (timing) CK(cudaEventRecordWithFlags(d.ev[4], s, cudaEventRecordExternal));
+    return GMAPF_OK;
+}
+
+int capture_graph(Context& c, std::string& err) {
+    Device& d = c.dev;
+    destroy_graph(c);
+    CK(cudaStreamBeginCapture(d.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_frame(c, c.cfg.IsProfiler != 0, err);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(d.stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        err = std::string("graph capture failed: ") + cudaGetErrorString(e);
+        return GMAPF_E_CUDA;
+    }
+    d.graph = g;
+    CK(cudaGraphInstantiate(&d.graph_exec, g, 0));
+    return GMAPF_OK;
+}
+
+int kernels_per_frame(Context& c) { return 2 + (c.A > 0 ? 4 : 0); }
+
+}  // namespace
+
+int device_start(Context& c, std::string& err) {
+    Device& d = c.dev;
+    d.device = c.opt.device;
+    CK(cudaSetDevice(d.device));
+    CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&d.stream2, cudaStreamNonBlocking));
+    for (auto& e : d.ev) CK(cudaEventCreate(&e));
+
+    const HostMap& m = c.map;
+    const int n = m.n;
+    // map
+    DALLOC(d.rows, n);
+    DALLOC(d.cen, n);
+    DALLOC(d.tri, 3 * (size_t)n);
+    DALLOC(d.gstart, m.gstart.size());
+    DALLOC(d.glist, m.glist.size());
+    DALLOC(d.degen, m.degen.size());
+    CK(cudaMemcpy(d.rows, m.rows.data(), sizeof(SearchRow) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.cen, m.cen.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.tri, m.tri.data(), sizeof(float2) * 3 * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.gstart, m.gstart.data(), sizeof(int) * m.gstart.size(), cudaMemcpyHostToDevice));
+    if (!m.glist.empty())
+        CK(cudaMemcpy(d.glist, m.glist.data(), sizeof(int) * m.glist.size(), cudaMemcpyHostToDevice));
+    if (!m.degen.empty())
+        CK(cudaMemcpy(d.degen, m.degen.data(), sizeof(int) * m.degen.size(), cudaMemcpyHostToDevice));
+
+    // agents
+    const int A = c.A;
+    DALLOC(d.pos, A);
+    DALLOC(d.pos_mid, A);
+    DALLOC(d.targ_pos, A);
+    DALLOC(d.step_pos, A);
+    DALLOC(d.state, A);
+    DALLOC(d.cur, A);
+    DALLOC(d.targ, A);
+    DALLOC(d.step_idx, A);
+    DALLOC(d.step_node, A);
+    DALLOC(d.path_len, A);
+    DALLOC(d.in_move, A);
+    DALLOC(d.dirty, A);
+    d.dirty_cap = A;
+    d.path_stride = std::max(1, n);
+    {
+        size_t freeb = 0, totalb = 0;
+        CK(cudaMemGetInfo(&freeb, &totalb));
+        double need = (double)std::max(1, A) * d.path_stride * sizeof(int);
+        if (need > 0.45 * (double)freeb) {
+            err = "path buffers (agents x triangles x 4 bytes = " + std::to_string((long long)need) +
+                  " bytes) exceed the device memory budget";
+            return GMAPF_E_CAPACITY;
+        }
+    }
+    DALLOC(d.paths, (size_t)std::max(1, A) * d.path_stride);
+    DALLOC(d.req, std::max(1, c.cfg.PathFinderParallelAgents));
+    DALLOC(d.counters, CT_COUNT);
+    DALLOC(d.stats, ST_COUNT);
+
+    std::vector<float2> tp(A);
+    std::vector<int> minus(A, -1);
+    for (int i = 0; i < A; i++) tp[i] = make_float2(c.m_targ[i].X, c.m_targ[i].Y);
+    if (A > 0) {
+        CK(cudaMemcpy(d.pos, c.m_pos.data(), sizeof(float2) * A, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.state, c.m_state.data(), sizeof(int) * A, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.cur, c.m_cur.data(), sizeof(int) * A, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.targ, c.m_targ_node.data(), sizeof(int) * A, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.targ_pos, tp.data(), sizeof(float2) * A, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.step_idx, minus.data(), sizeof(int) * A, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.step_node, minus.data(), sizeof(int) * A, cudaMemcpyHostToDevice));
+    }
+
+    // agent grid
+    MoverParams mp = mover_params(c);
+    d.cells = mp.aw * mp.ah;
+    DALLOC(d.cell_of, A);
+    DALLOC(d.cell_cnt, (size_t)d.cells + 1);
+    DALLOC(d.cell_start, (size_t)d.cells + 1);
+    DALLOC(d.cell_fill, (size_t)d.cells + 1);
+    DALLOC(d.cell_items, A);
+
+    // pinned host staging
+    CK(cudaMallocHost((void**)&c.h_pos_stage, sizeof(float2) * std::max(1, A)));
+    CK(cudaMallocHost((void**)&c.h_state_stage, sizeof(int) * std::max(1, A)));
+    CK(cudaMallocHost((void**)&c.h_dirty, sizeof(int4) * std::max(1, A)));
+    CK(cudaMallocHost((void**)&c.h_small, sizeof(int) * CT_COUNT));
+    CK(cudaMallocHost((void**)&c.h_stats, sizeof(unsigned long long) * ST_COUNT));
+    CK(cudaMallocHost((void**)&c.h_step, sizeof(float) * 4));
+    std::memset(c.h_stats, 0, sizeof(unsigned long long) * ST_COUNT);
+
+    int rc = alloc_search_state(c, err);
+    if (rc) return rc;
+    CK(cudaDeviceSynchronize());
+    return GMAPF_OK;
+}
+
+void device_free(Context& c) {
+    Device& d = c.dev;
+    if (d.stream) cudaStreamSynchronize(d.stream);
+    if (d.stream2) cudaStreamSynchronize(d.stream2);
+    destroy_graph(c);
+    for (void* p : d.allocs)
+        if (p) cudaFree(p);
+    d.allocs.clear();
+    for (auto& e : d.ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    if (d.stream) cudaStreamDestroy(d.stream);
+    if (d.stream2) cudaStreamDestroy(d.stream2);
+    d.stream = d.stream2 = nullptr;
+    void* hp[] = {c.h_pos_stage, c.h_state_stage, c.h_dirty, c.h_small, c.h_stats, c.h_step};
+    for (void* p : hp)
+        if (p) cudaFreeHost(p);
+    c.h_pos_stage = nullptr;
+    c.h_state_stage = nullptr;
+    c.h_dirty = nullptr;
+    c.h_small = nullptr;
+    c.h_stats = nullptr;
+    c.h_step = nullptr;
+}
+
+int device_async_step(Context& c, float dt, std::string& err) {
+    Device& d = c.dev;
+    cudaStream_t s = d.stream;
+    CK(cudaSetDevice(d.device));
+    c.t_step0 = std::chrono::steady_clock::now();
+    // changed targets (src/GMAPF.cu:270-278 copies the whole agent array)
+    const int nd = (int)c.dirty_recs.size();
+    c.pre_done = nd > 0;
+    if (nd > 0) {
+        std::memcpy(c.h_dirty, c.dirty_recs.data(), sizeof(int4) * nd);
+        CK(cudaMemcpyAsync(d.dirty, c.h_dirty, sizeof(int4) * nd, cudaMemcpyHostToDevice, s));
+        launch_apply_targets(s, d.dirty, nd, d.state, d.targ, d.targ_pos);
+        c.launches += 1;
+        for (const int4& r : c.dirty_recs) c.dirty_slot[r.x] = -1;
+        c.dirty_recs.clear();
+    }
+    c.h_step[0] = c.cfg.AgentSpeed * dt;
+    CK(cudaMemcpyAsync(d.counters + 8, c.h_step, sizeof(float), cudaMemcpyHostToDevice, s));
+
+    if (c.opt.mode == GMAPF_MODE_BATCHED) {
+        if (!d.graph_exec) {
+            int rc = capture_graph(c, err);
+            if (rc) return rc;
+        }
+        CK(cudaGraphLaunch(d.graph_exec, s));
+        c.launches += kernels_per_frame(c);
+    } else {
+        // plain: the reference's shape -- counts read back mid-frame
+        const bool timing = c.cfg.IsProfiler != 0;
+        if (timing) CK(cudaEventRecord(d.ev[0], s));
+        CK(cudaMemsetAsync(d.counters + CT_ERR, 0, sizeof(int), s));
+        launch_compact(s, c.A, d.state, d.cur, d.targ, c.cfg.PathFinderParallelAgents, d.req,
+                       d.counters + CT_REQ, d.in_move, d.counters + CT_MOVE, d.counters + CT_WORK,
+                       d.stats);
+        c.launches += 1;
+        CK(cudaMemcpyAsync(c.h_small, d.counters, sizeof(int) * CT_COUNT, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (timing) CK(cudaEventRecord(d.ev[1], s));
+        const int R = c.h_small[CT_REQ], M = c.h_small[CT_MOVE];
+        c.plain_req_count = R;
+        c.plain_mv_count = M;
+        if (R > 0) {
+            SearchParams sp = search_params(c);
+            sp.req_count_h = R;
+            const int chunk = d.slots;
+            for (int base = 0; base < R; base += chunk) {
+                const int cnt = std::min(chunk, R - base);
+                const int gpb = c.block_threads / c.T;
+                const int blocks = (cnt + gpb - 1) / gpb;
+                CK(launch_search(s, sp, blocks, c.block_threads, false, base));
+                c.launches += 1;
+            }
+        }
+        if (timing) CK(cudaEventRecord(d.ev[2], s));
+        if (M > 0) {
+            MoverParams mp = mover_params(c);
+            CK(cudaMemsetAsync(d.cell_cnt, 0, sizeof(int) * (d.cells + 1), s));
+            launch_move_bin(s, mp);
+            launch_cell_scan(s, mp);
+            launch_scatter(s, mp);
+            launch_collide_progress(s, mp);
+            c.launches += 4;
+        }
+        if (timing) CK(cudaEventRecord(d.ev[3], s));
+        if (c.A > 0) {
+            CK(cudaMemcpyAsync(c.h_pos_stage, d.pos, sizeof(float2) * c.A, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(c.h_state_stage, d.state, sizeof(int) * c.A, cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaMemcpyAsync(c.h_small, d.counters, sizeof(int) * CT_COUNT, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(c.h_stats, d.stats, sizeof(unsigned long long) * ST_COUNT, cudaMemcpyDeviceToHost, s));
+        if (timing) CK(cudaEventRecord(d.ev[4], s));
+    }
+    return GMAPF_OK;
+}
+
+int device_wait_step(Context& c, std::string& err) {
+    Device& d = c.dev;
+    CK(cudaSetDevice(d.device));
+    CK(cudaStreamSynchronize(d.stream));
+    const auto t1 = std::chrono::steady_clock::now();
+    if (c.A > 0) {
+        for (int i = 0; i < c.A; i++) {
+            c.m_pos[i].X = c.h_pos_stage[i].x;
+            c.m_pos[i].Y = c.h_pos_stage[i].y;
+        }
+        std::memcpy(c.m_state.data(), c.h_state_stage, sizeof(int) * c.A);
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    unsigned long long delta[ST_COUNT];
+    for (int k = 0; k < ST_COUNT; k++) {
+        delta[k] = c.h_stats[k] - c.stats_prev[k];
+        c.stats_prev[k] = c.h_stats[k];
+    }
+    gmapf_step_stats& st = c.last;
+    st.requests = (int64_t)delta[ST_REQUESTS];
+    st.found = (int64_t)delta[ST_FOUND];
+    st.expansions = (int64_t)delta[ST_EXPANSIONS];
+    st.rounds = (int64_t)delta[ST_ROUNDS];
+    st.deg_sum = (int64_t)delta[ST_DEG_SUM];
+    st.claims = (int64_t)delta[ST_CLAIMS];
+    st.path_nodes = (int64_t)delta[ST_PATH_NODES];
+    st.moving = (int64_t)delta[ST_MOVING];
+    st.ms_step_wall = std::chrono::duration<float, std::milli>(t2 - c.t_step0).count();
+    st.ms_search = st.ms_mover = st.ms_total_device = 0;
+    if (c.cfg.IsProfiler) {
+        float a = 0, b = 0, t = 0, cp = 0;
+        cudaEventElapsedTime(&cp, d.ev[0], d.ev[1]);
+        cudaEventElapsedTime(&a, d.ev[1], d.ev[2]);
+        cudaEventElapsedTime(&b, d.ev[c.opt.mode == GMAPF_MODE_BATCHED ? 1 : 2], d.ev[3]);
+        cudaEventElapsedTime(&t, d.ev[0], d.ev[4]);
+        cudaGetLastError();
+        st.ms_search = a;
+        st.ms_mover = b;
+        st.ms_total_device = t;
+        Profiler& p = c.prof;
+        p.n++;
+        p.sum_wall += st.ms_step_wall;
+        p.max_wall = std::max(p.max_wall, st.ms_step_wall);
+        p.sum_compact += cp;
+        p.max_compact = std::max(p.max_compact, cp);
+        if (st.requests > 0) {
+            p.n_search++;
+            p.sum_search += a;
+            p.max_search = std::max(p.max_search, a);
+        }
+        if (st.moving > 0) {
+            p.n_mover++;
+            p.sum_mover += b;
+            p.max_mover = std::max(p.max_mover, b);
+        }
+        const float post = std::chrono::duration<float, std::milli>(t2 - t1).count();
+        p.sum_post += post;
+        p.max_post = std::max(p.max_post, post);
+    }
+    c.prof.wall_ms.push_back(st.ms_step_wall);
+    const int e = c.h_small[CT_ERR];
+    if (e != 0) {
+        err = "device-side check failed (error bits " + std::to_string(e) + ")";
+        return GMAPF_E_DEVICE;
+    }
+    return GMAPF_OK;
+}
+
+int device_search_batch(Context& c, const int* d_starts, const int* d_targets, int n, int* d_found,
+                        int* d_lens, int* d_paths, long long path_stride, gmapf_step_stats* out,
+                        std::string& err) {
+    Device& d = c.dev;
+    cudaStream_t s = d.stream;
+    CK(cudaSetDevice(d.device));
+    if (n > d.breq_cap) {
+        if (d.breq) {
+            cudaFree(d.breq);
+            d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), (void*)d.breq), d.allocs.end());
+        }
+        d.breq = nullptr;
+        DALLOC(d.breq, (size_t)n);
+        d.breq_cap = n;
+    }
+    CK(cudaMemsetAsync(d.counters + CT_ERR, 0, sizeof(int), s));
+    CK(cudaMemcpyAsync(c.h_stats, d.stats, sizeof(unsigned long long) * ST_COUNT, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    unsigned long long before[ST_COUNT];
+    std::memcpy(before, c.h_stats, sizeof(before));
+    launch_prepare_batch(s, d_starts, d_targets, n, c.map.n, d.breq, d.counters + CT_REQ,
+                         d.counters + CT_WORK, d.counters + CT_ERR);
+    c.launches += 1;
+    SearchParams sp = search_params(c);
+    sp.req = d.breq;
+    sp.paths = d_paths;
+    sp.path_stride = path_stride;
+    sp.out_found = d_found;
+    sp.out_len = d_lens;
+    sp.ag_state = nullptr;
+    sp.ag_step_idx = nullptr;
+    sp.ag_path_len = nullptr;
+    CK(cudaEventRecord(d.ev[6], s));
+    if (n > 0) {
+        if (c.opt.mode == GMAPF_MODE_BATCHED) {
+            CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0));
+            c.launches += 1;
+        } else {
+            sp.req_count_h = n;
+            const int gpb = c.block_threads / c.T;
+            for (int base = 0; base < n; base += d.slots) {
+                const int cnt = std::min(d.slots, n - base);
+                CK(launch_search(s, sp, (cnt + gpb - 1) / gpb, c.block_threads, false, base));
+                c.launches += 1;
+            }
+        }
+    }
+    CK(cudaEventRecord(d.ev[7], s));
+    CK(cudaMemcpyAsync(c.h_small, d.counters, sizeof(int) * CT_COUNT, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(c.h_stats, d.stats, sizeof(unsigned long long) * ST_COUNT, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, d.ev[6], d.ev[7]));
+    c.last_search_ms = ms;
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->requests = n;
+        out->found = (int64_t)(c.h_stats[ST_FOUND] - before[ST_FOUND]);
+        out->expansions = (int64_t)(c.h_stats[ST_EXPANSIONS] - before[ST_EXPANSIONS]);
+        out->rounds = (int64_t)(c.h_stats[ST_ROUNDS] - before[ST_ROUNDS]);
+        out->deg_sum = (int64_t)(c.h_stats[ST_DEG_SUM] - before[ST_DEG_SUM]);
+        out->claims = (int64_t)(c.h_stats[ST_CLAIMS] - before[ST_CLAIMS]);
+        out->path_nodes = (int64_t)(c.h_stats[ST_PATH_NODES] - before[ST_PATH_NODES]);
+        out->ms_search = ms;
+        out->ms_total_device = ms;
+    }
+    // keep the step's delta base consistent with the searches done here
+    for (int k = 0; k < ST_COUNT; k++) c.stats_prev[k] += c.h_stats[k] - before[k];
+    const int e = c.h_small[CT_ERR];
+    if (e != 0) {
+        err = "device-side check failed (error bits " + std::to_string(e) + ")";
+        return (e & ERR_BAD_REQUEST) ? GMAPF_E_INVALID_ARG : GMAPF_E_DEVICE;
+    }
+    return GMAPF_OK;
+}
+
+int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err) {
+    Device& d = c.dev;
+    if (n > d.bio_cap || (long long)n * path_stride > d.bpaths_cap) {
+        void* old[] = {d.bstarts, d.btargets, d.bfound, d.blens, d.bpaths};
+        for (void* p : old) {
+            if (!p) continue;
+            cudaFree(p);
+            d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), p), d.allocs.end());
+        }
+        d.bstarts = d.btargets = d.bfound = d.blens = d.bpaths = nullptr;
+        DALLOC(d.bstarts, (size_t)n);
+        DALLOC(d.btargets, (size_t)n);
+        DALLOC(d.bfound, (size_t)n);
+        DALLOC(d.blens, (size_t)n);
+        DALLOC(d.bpaths, (size_t)n * path_stride);
+        d.bio_cap = n;
+        d.bpaths_cap = (long long)n * path_stride;
+    }
+    return GMAPF_OK;
+}
+
+int device_debug_agents(Context& c, gmapf_v2* pos, int* state, int* cur, int* targ, int* step_idx,
+                        int* step_node, gmapf_v2* step_pos, int* path_len, std::string& err) {
+    Device& d = c.dev;
+    const int A = c.A;
+    CK(cudaSetDevice(d.device));
+    CK(cudaStreamSynchronize(d.stream));
+    if (A == 0) return GMAPF_OK;
+    if (pos) CK(cudaMemcpy(pos, d.pos, sizeof(float2) * A, cudaMemcpyDeviceToHost));
+    if (state) CK(cudaMemcpy(state, d.state, sizeof(int) * A, cudaMemcpyDeviceToHost));
+    if (cur) CK(cudaMemcpy(cur, d.cur, sizeof(int) * A, cudaMemcpyDeviceToHost));
+    if (targ) CK(cudaMemcpy(targ, d.targ, sizeof(int) * A, cudaMemcpyDeviceToHost));
+    if (step_idx) CK(cudaMemcpy(step_idx, d.step_idx, sizeof(int) * A, cudaMemcpyDeviceToHost));
+    if (step_node) CK(cudaMemcpy(step_node, d.step_node, sizeof(int) * A, cudaMemcpyDeviceToHost));
+    if (step_pos) CK(cudaMemcpy(step_pos, d.step_pos, sizeof(float2) * A, cudaMemcpyDeviceToHost));
+    if (path_len) CK(cudaMemcpy(path_len, d.path_len, sizeof(int) * A, cudaMemcpyDeviceToHost));
+    return GMAPF_OK;
+}
+
+int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::string& err) {
+    Device& d = c.dev;
+    CK(cudaSetDevice(d.device));
+    CK(cudaStreamSynchronize(d.stream));
+    int L = 0;
+    CK(cudaMemcpy(&L, d.path_len + id, sizeof(int), cudaMemcpyDeviceToHost));
+    *out_len = L;
+    const int k = std::min(L, cap);
+    if (k > 0) CK(cudaMemcpy(out, d.paths + (long long)id * d.path_stride, sizeof(int) * k, cudaMemcpyDeviceToHost));
+    return GMAPF_OK;
+}
+
+// Re-size the search state after the search parameters change (autotuner).
+int device_reconfigure_search(Context& c, std::string& err) {
+    destroy_graph(c);
+    free_search_state(c);
+    return alloc_search_state(c, err);
+}
+
+int device_autotune(Context& c, std::string& err) {
+    (void)c;
+    (void)err;
+    return GMAPF_OK;
+}
+
+}  // namespace gmapf_b200

@@ -1,0 +1,266 @@
+// internal.h -- host-side structures of the B200 G-MAPF library (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gmapf_c.h"
+#include "geom.cuh"
+
+namespace gmapf_b200 {
+
+// ------------------------------------------------------------------ device --
+
+// Per-slot visited record of one claimed node, 32 bytes.  `stamp` equals the
+// slot's current query epoch iff the node is claimed by that query, so slots
+// are reused across queries and frames without clearing.  `gd` = G << 1 | dir
+// (dir 1 = reached from the start, PathNode::FromStart).  anc[0] is the
+// parent (PathNode::PrevNodeIdx); anc[k] the (k+1)-th ancestor, so a path
+// walk advances six hops per record read.
+struct __align__(16) Rec {
+    unsigned stamp;
+    int gd;
+    int anc[6];
+};
+
+enum StatIdx {
+    ST_EXPANSIONS = 0,
+    ST_ROUNDS,
+    ST_DEG_SUM,
+    ST_CLAIMS,
+    ST_PATH_NODES,
+    ST_FOUND,
+    ST_REQUESTS,
+    ST_MOVING,
+    ST_COUNT
+};
+
+enum ErrBits {
+    ERR_BOUNDS = 1,      // an index failed its bounds check (access skipped)
+    ERR_ROUNDS = 2,      // a search exceeded its round limit
+    ERR_PATH_CAP = 4,    // a path did not fit its output row
+    ERR_BAD_REQUEST = 8  // a request named a node outside the map
+};
+
+struct SearchParams {
+    const SearchRow* rows;
+    const float2* cen;
+    int n;
+    const int4* req;         // {agent (or -1), start, target, output row}
+    const int* req_count_d;  // device count (persistent form)
+    int req_count_h;         // host count (plain form)
+    int T, C;
+    float K;
+    Rec* rec;                // slots * n
+    unsigned* epoch;         // per slot
+    int slots;
+    int* work_ctr;
+    int max_rounds;
+    // outputs
+    int* paths;              // row-major, path_stride ints per row
+    long long path_stride;
+    int* out_found;          // per request (batch API) or null
+    int* out_len;            // per request (batch API) or null
+    int* ag_state;           // agent arrays (step) or null
+    int* ag_step_idx;
+    int* ag_path_len;
+    unsigned long long* stats;  // ST_COUNT counters
+    int* err;
+};
+
+struct MoverParams {
+    int A;
+    const int* mv_count;
+    const unsigned char* in_move;
+    float2* pos;       // in: previous frame, out: final (collision output)
+    float2* pos_mid;   // after move (collision snapshot)
+    float2* step_pos;
+    const float2* targ_pos;
+    int* state;
+    int* cur_node;
+    int* step_idx;
+    int* step_node;
+    const int* path_len;
+    const int* paths;
+    long long path_stride;
+    const float* step; // speed * dt (device scalar, set per frame)
+    float cd, cd2;     // collision distance and its square
+    float arrive;      // FLT_EPSILON + radius
+    float cs, sn;      // rotation by +10 degrees
+    // agent grid
+    float ax0, ay0, ainv;
+    int aw, ah;
+    int* cell_of;
+    int* cell_cnt;     // aw*ah + 1
+    int* cell_start;   // aw*ah + 1
+    int* cell_fill;    // aw*ah
+    int* cell_items;   // A
+    // map
+    LocateGrid loc;
+    const float2* cen;
+    int n;
+    unsigned long long* stats;
+    int* err;
+};
+
+// kernels.cu
+void launch_compact(cudaStream_t s, int A, int* state, const int* cur, const int* targ, int P,
+                    int4* req, int* req_count, unsigned char* in_move, int* mv_count, int* work_ctr,
+                    unsigned long long* stats);
+void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, int* targ_node,
+                          float2* targ_pos);
+void launch_move_bin(cudaStream_t s, const MoverParams& p);
+void launch_cell_scan(cudaStream_t s, const MoverParams& p);
+void launch_scatter(cudaStream_t s, const MoverParams& p);
+void launch_collide_progress(cudaStream_t s, const MoverParams& p);
+void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets, int n, int nodes,
+                          int4* req, int* req_count, int* work_ctr, int* err);
+// search.cu
+// persistent: groups pull requests from *work_ctr until *req_count_d is reached.
+// plain: one request per group, requests [base, base + groups).
+cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int block_threads,
+                          bool persistent, int req_base);
+size_t search_smem_bytes(int T, int C, int block_threads);
+int search_max_blocks_per_sm(int T, int C, int block_threads);
+
+// ------------------------------------------------------------------- host --
+
+struct HostMap {
+    int n = 0;
+    std::vector<gmapf_node> nodes;  // as ingested, PCenter recomputed
+    std::vector<SearchRow> rows;
+    std::vector<float2> tri;        // 3 per node
+    std::vector<float2> cen;
+    float bx0 = 0, by0 = 0, bx1 = 0, by1 = 0;
+    float gx0 = 0, gy0 = 0, ginv = 1;
+    int gw = 1, gh = 1;
+    std::vector<int> gstart, glist, degen;
+    LocateGrid view() const;
+};
+
+// hostmap.cpp
+void build_host_map(const gmapf_node* nodes, int n, HostMap& out);
+// navmesh_cdt.cpp: 0 on success, else a gmapf_status with `err` set
+int build_navmesh_cdt(const std::vector<float>& verts, const std::vector<unsigned>& edges,
+                      std::vector<gmapf_node>& out, std::string& err);
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Device {
+    int device = 0;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    // map
+    SearchRow* rows = nullptr;
+    float2* cen = nullptr;
+    float2* tri = nullptr;
+    int *gstart = nullptr, *glist = nullptr, *degen = nullptr;
+    // agents
+    float2 *pos = nullptr, *pos_mid = nullptr, *targ_pos = nullptr, *step_pos = nullptr;
+    int *state = nullptr, *cur = nullptr, *targ = nullptr, *step_idx = nullptr, *step_node = nullptr,
+        *path_len = nullptr;
+    int* paths = nullptr;
+    long long path_stride = 0;
+    unsigned char* in_move = nullptr;
+    int4* dirty = nullptr;
+    int dirty_cap = 0;
+    // requests / counters
+    int4* req = nullptr;
+    int* counters = nullptr;  // [req_count, mv_count, work_ctr, err, spare...]
+    unsigned long long* stats = nullptr;
+    // search state
+    Rec* rec = nullptr;
+    unsigned* epoch = nullptr;
+    int slots = 0;
+    // agent grid
+    int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
+        *cell_items = nullptr;
+    int cells = 0;
+    // batch API scratch
+    int4* breq = nullptr;
+    int breq_cap = 0;
+    int *bstarts = nullptr, *btargets = nullptr, *bfound = nullptr, *blens = nullptr,
+        *bpaths = nullptr;
+    long long bpaths_cap = 0;
+    int bio_cap = 0;
+    // graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    float graph_dt = -1.0f;
+    // events
+    cudaEvent_t ev[8] = {};
+    std::vector<void*> allocs;
+};
+
+struct Profiler {
+    std::vector<float> wall_ms;
+    float sum_wall = 0, max_wall = 0;
+    float sum_pre = 0, max_pre = 0;
+    int n_pre = 0;
+    float sum_post = 0, max_post = 0;
+    float sum_search = 0, max_search = 0;
+    float sum_mover = 0, max_mover = 0;
+    float sum_compact = 0, max_compact = 0;
+    int n = 0, n_search = 0, n_mover = 0;
+};
+
+struct Context {
+    bool inited = false, started = false, step_going = false;
+    gmapf_config cfg{};
+    gmapf_options opt{};
+    // map ingestion
+    std::vector<float> cdt_v;
+    std::vector<unsigned> cdt_e;
+    bool map_filled = false;
+    HostMap map;
+    // agents: host mirror (capacity reserved at Init, so pointers stay valid)
+    int A = 0;
+    std::vector<gmapf_v2> m_pos;
+    std::vector<int> m_state, m_cur, m_targ_node;
+    std::vector<gmapf_v2> m_targ;
+    // pinned staging (allocated at start)
+    float2* h_pos_stage = nullptr;
+    int* h_state_stage = nullptr;
+    int4* h_dirty = nullptr;
+    int* h_small = nullptr;            // counters snapshot
+    unsigned long long* h_stats = nullptr;
+    float* h_step = nullptr;
+    std::vector<int4> dirty_recs;
+    std::vector<int> dirty_slot;       // agent -> index in dirty_recs or -1
+    // effective search parameters
+    int T = 4, C = 16, block_threads = 128;
+    float K = 1.0f;
+    // device
+    Device dev;
+    Profiler prof;
+    gmapf_step_stats last{};
+    unsigned long long stats_prev[ST_COUNT] = {};
+    std::chrono::steady_clock::time_point t_step0;
+    float pre_ms = 0;
+    bool pre_done = false;
+    long long launches = 0;
+    float last_search_ms = 0;
+    int plain_req_count = 0, plain_mv_count = 0;
+};
+
+// device.cu
+int device_start(Context& c, std::string& err);
+void device_free(Context& c);
+int device_async_step(Context& c, float dt, std::string& err);
+int device_wait_step(Context& c, std::string& err);
+int device_search_batch(Context& c, const int* d_starts, const int* d_targets, int n, int* d_found,
+                        int* d_lens, int* d_paths, long long path_stride, gmapf_step_stats* st,
+                        std::string& err);
+int device_debug_agents(Context& c, gmapf_v2* pos, int* state, int* cur, int* targ, int* step_idx,
+                        int* step_node, gmapf_v2* step_pos, int* path_len, std::string& err);
+int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::string& err);
+int device_autotune(Context& c, std::string& err);
+int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
+
+}  // namespace gmapf_b200

@@ -1,0 +1,365 @@
+// kernels.cu -- request compaction, target upload and the agents mover.
+//
+// Reference kernels restated here:
+//   KernelFindRequests        include/gmapf/PathFinder.h:76-117
+//   KernelFindMovingAgents    include/gmapf/AgentsMover.h:29-49
+//   KernelMoveAgents          include/gmapf/AgentsMover.h:51-71
+//   KernelResolveCollisions   include/gmapf/AgentsMover.h:73-129
+//   KernelUpdatePathProgress  include/gmapf/AgentsMover.h:131-177
+// Agents are stored as structure-of-arrays.  Compaction is stable (requests
+// in ascending agent id).  Collisions read one snapshot of the positions
+// after the move and write a second buffer (Jacobi); each agent sums its
+// contributions in ascending neighbour id, found through a counting-sort
+// uniform grid whose cells are at least 1.0625 collision distances wide, so
+// the 3x3 neighbourhood holds every agent the reference's all-pairs loop
+// would accept.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace gmapf_b200 {
+
+namespace {
+
+constexpr int kCompactThreads = 1024;
+
+__global__ void __launch_bounds__(kCompactThreads)
+    k_compact(int A, int* state, const int* cur, const int* targ, int P, int4* req, int* req_count,
+              unsigned char* in_move, int* mv_count, int* work_ctr, unsigned long long* stats) {
+    __shared__ int warp_tot[32];
+    __shared__ int warp_totm[32];
+    __shared__ int base_s, base_m;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        base_s = 0;
+        base_m = 0;
+    }
+    __syncthreads();
+    for (int b = 0; b < A; b += kCompactThreads) {
+        const int i = b + tid;
+        bool isS = false, isM = false;
+        int cu = 0, ta = 0;
+        if (i < A) {
+            const int st = state[i];
+            if (st == GMAPF_AGENT_SEARCH) {
+                cu = cur[i];
+                ta = targ[i];
+                if (cu == ta) {
+                    state[i] = GMAPF_AGENT_IDLE;  // PathFinder.h:91-95
+                } else {
+                    isS = true;
+                }
+            }
+            isM = st == GMAPF_AGENT_MOVE;
+            in_move[i] = isM ? 1 : 0;
+        }
+        const unsigned bs = __ballot_sync(0xffffffffu, isS);
+        const unsigned bm = __ballot_sync(0xffffffffu, isM);
+        if (lane == 0) {
+            warp_tot[warp] = __popc(bs);
+            warp_totm[warp] = __popc(bm);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            int v = warp_tot[lane], vm = warp_totm[lane];
+            // inclusive scans over the 32 warp totals
+            for (int o = 1; o < 32; o <<= 1) {
+                int t = __shfl_up_sync(0xffffffffu, v, o);
+                int tm = __shfl_up_sync(0xffffffffu, vm, o);
+                if (lane >= o) {
+                    v += t;
+                    vm += tm;
+                }
+            }
+            warp_tot[lane] = v;  // inclusive
+            warp_totm[lane] = vm;
+        }
+        __syncthreads();
+        const int wpre = (warp == 0) ? 0 : warp_tot[warp - 1];
+        if (isS) {
+            const int pos = base_s + wpre + __popc(bs & ((1u << lane) - 1u));
+            if (pos < P) req[pos] = make_int4(i, cu, ta, i);  // over capacity: stays Search
+        }
+        __syncthreads();
+        if (tid == 0) {
+            base_s += warp_tot[31];
+            base_m += warp_totm[31];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const int R = base_s < P ? base_s : P;
+        *req_count = R;
+        *mv_count = base_m;
+        *work_ctr = 0;
+        stats[ST_REQUESTS] += (unsigned long long)R;
+        stats[ST_MOVING] += (unsigned long long)base_m;
+    }
+}
+
+__global__ void k_apply_targets(const int4* recs, int n, int* state, int* targ_node,
+                                float2* targ_pos) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int4 r = recs[k];  // {agent, node, x bits, y bits}
+    state[r.x] = GMAPF_AGENT_SEARCH;
+    targ_node[r.x] = r.y;
+    targ_pos[r.x] = make_float2(__int_as_float(r.z), __int_as_float(r.w));
+}
+
+__global__ void k_prepare_batch(const int* starts, const int* targets, int n, int nodes, int4* req,
+                                int* req_count, int* work_ctr, int* err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) {
+        *req_count = n;
+        *work_ctr = 0;
+    }
+    if (k >= n) return;
+    int s = starts[k], t = targets[k];
+    if (s < 0 || s >= nodes || t < 0 || t >= nodes) atomicOr(err, ERR_BAD_REQUEST);
+    req[k] = make_int4(-1, s, t, k);
+}
+
+// move (AgentsMover.h:51-71) fused with the agent-grid histogram
+__global__ void k_move_bin(MoverParams p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (*p.mv_count == 0) return;  // AgentsMover.h:296-297
+    if (i >= p.A) return;
+    float2 c = p.pos[i];
+    const float step = *p.step;
+    if (p.in_move[i] && p.step_idx[i] != -1) {
+        const float2 s = p.step_pos[i];
+        const float dx = GM_FSUB(s.x, c.x), dy = GM_FSUB(s.y, c.y);
+        const float len = GM_FSQRT(GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy)));
+        if (len <= step) {
+            c = s;
+        } else {
+            c.x = GM_FADD(c.x, GM_FMUL(GM_FDIV(dx, len), step));
+            c.y = GM_FADD(c.y, GM_FMUL(GM_FDIV(dy, len), step));
+        }
+    }
+    p.pos_mid[i] = c;
+    int cell = -1;
+    if (gm_isfinite(c.x) && gm_isfinite(c.y)) {
+        const int cx = grid_cell(c.x, p.ax0, p.ainv, p.aw);
+        const int cy = grid_cell(c.y, p.ay0, p.ainv, p.ah);
+        cell = cy * p.aw + cx;
+        atomicAdd(p.cell_cnt + cell, 1);
+    }
+    p.cell_of[i] = cell;
+}
+
+// exclusive scan of the cell histogram, one block
+__global__ void __launch_bounds__(1024) k_cell_scan(MoverParams p) {
+    if (*p.mv_count == 0) return;
+    __shared__ int part[1024];
+    const int cells = p.aw * p.ah;
+    const int tid = threadIdx.x;
+    const int per = (cells + 1023) / 1024;
+    const int b = tid * per, e = min(b + per, cells);
+    int s = 0;
+    for (int k = b; k < e; k++) s += p.cell_cnt[k];
+    part[tid] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int v = (tid >= o) ? part[tid - o] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int run = (tid == 0) ? 0 : part[tid - 1];
+    for (int k = b; k < e; k++) {
+        p.cell_start[k] = run;
+        p.cell_fill[k] = run;
+        run += p.cell_cnt[k];
+    }
+    if (tid == 1023) p.cell_start[cells] = part[1023];
+}
+
+__global__ void k_scatter(MoverParams p) {
+    if (*p.mv_count == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.A) return;
+    const int c = p.cell_of[i];
+    if (c < 0) return;
+    const int k = atomicAdd(p.cell_fill + c, 1);
+    p.cell_items[k] = i;
+}
+
+constexpr int kMaxLocal = 16;
+
+// collisions (AgentsMover.h:73-129) + path progress (AgentsMover.h:131-177)
+__global__ void k_collide_progress(MoverParams p) {
+    if (*p.mv_count == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.A) return;
+    const float2 me = p.pos_mid[i];
+    float2 np = me;
+    const int c = p.cell_of[i];
+    if (c >= 0) {
+        const int cx = c % p.aw, cy = c / p.aw;
+        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, p.aw - 1);
+        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, p.ah - 1);
+        int ids[kMaxLocal];
+        float vxs[kMaxLocal], vys[kMaxLocal];
+        int cnt = 0;
+        bool overflow = false;
+        for (int yy = y0; yy <= y1; yy++)
+            for (int xx = x0; xx <= x1; xx++) {
+                const int cc = yy * p.aw + xx;
+                for (int k = p.cell_start[cc], e = p.cell_start[cc + 1]; k < e; k++) {
+                    const int j = p.cell_items[k];
+                    if (j == i) continue;
+                    const float2 o = p.pos_mid[j];
+                    const float dx = GM_FSUB(me.x, o.x), dy = GM_FSUB(me.y, o.y);
+                    const float d2 = GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy));
+                    if (!(d2 < p.cd2)) continue;
+                    if (cnt >= kMaxLocal) {
+                        overflow = true;
+                        continue;
+                    }
+                    const float d = GM_FSQRT(d2);
+                    const float shift = GM_FSUB(p.cd, d);
+                    const float vx = GM_FMUL(GM_FDIV(dx, d), shift);
+                    const float vy = GM_FMUL(GM_FDIV(dy, d), shift);
+                    // insertion keeps ids ascending
+                    int k2 = cnt++;
+                    while (k2 > 0 && ids[k2 - 1] > j) {
+                        ids[k2] = ids[k2 - 1];
+                        vxs[k2] = vxs[k2 - 1];
+                        vys[k2] = vys[k2 - 1];
+                        k2--;
+                    }
+                    ids[k2] = j;
+                    vxs[k2] = vx;
+                    vys[k2] = vy;
+                }
+            }
+        float sx = 0.f, sy = 0.f;
+        int total = 0;
+        if (!overflow) {
+            for (int k = 0; k < cnt; k++) {
+                sx = GM_FADD(sx, vxs[k]);
+                sy = GM_FADD(sy, vys[k]);
+            }
+            total = cnt;
+        } else {
+            // dense crowd: take contributors in ascending id by repeated minimum search
+            int last = -1;
+            for (;;) {
+                int best = 0x7fffffff;
+                float bvx = 0.f, bvy = 0.f;
+                for (int yy = y0; yy <= y1; yy++)
+                    for (int xx = x0; xx <= x1; xx++) {
+                        const int cc = yy * p.aw + xx;
+                        for (int k = p.cell_start[cc], e = p.cell_start[cc + 1]; k < e; k++) {
+                            const int j = p.cell_items[k];
+                            if (j == i || j <= last || j >= best) continue;
+                            const float2 o = p.pos_mid[j];
+                            const float dx = GM_FSUB(me.x, o.x), dy = GM_FSUB(me.y, o.y);
+                            const float d2 = GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy));
+                            if (!(d2 < p.cd2)) continue;
+                            const float d = GM_FSQRT(d2);
+                            const float shift = GM_FSUB(p.cd, d);
+                            best = j;
+                            bvx = GM_FMUL(GM_FDIV(dx, d), shift);
+                            bvy = GM_FMUL(GM_FDIV(dy, d), shift);
+                        }
+                    }
+                if (best == 0x7fffffff) break;
+                sx = GM_FADD(sx, bvx);
+                sy = GM_FADD(sy, bvy);
+                total++;
+                last = best;
+            }
+        }
+        if (total > 0) {
+            const float fc = (float)total;
+            const float ax = GM_FDIV(sx, fc), ay = GM_FDIV(sy, fc);
+            const float rx = GM_FSUB(GM_FMUL(ax, p.cs), GM_FMUL(ay, p.sn));
+            const float ry = GM_FADD(GM_FMUL(ax, p.sn), GM_FMUL(ay, p.cs));
+            const float px = GM_FADD(me.x, rx), py = GM_FADD(me.y, ry);
+            if (locate(p.loc, px, py) >= 0) np = make_float2(px, py);
+        }
+    }
+    p.pos[i] = np;
+
+    if (!p.in_move[i]) return;
+    // path progress
+    const int* path = p.paths + (long long)i * p.path_stride;
+    const int L = p.path_len[i];
+    int si = p.step_idx[i];
+    if (si == -1) {
+        if (L < 1) {
+            atomicOr(p.err, ERR_BOUNDS);
+            return;
+        }
+        const int nd = path[0];
+        p.step_idx[i] = 0;
+        p.step_node[i] = nd;
+        p.step_pos[i] = p.cen[nd];
+        return;
+    }
+    const int sn = p.step_node[i];
+    if (sn < 0 || sn >= p.n) {
+        atomicOr(p.err, ERR_BOUNDS);
+        return;
+    }
+    if (!point_in_tri(np.x, np.y, p.loc.tri[3 * sn], p.loc.tri[3 * sn + 1], p.loc.tri[3 * sn + 2]))
+        return;
+    p.cur_node[i] = sn;
+    if (si < L) si += 1;
+    p.step_idx[i] = si;
+    if (si == L) {
+        const float2 t = p.targ_pos[i];
+        const float dx = GM_FSUB(t.x, np.x), dy = GM_FSUB(t.y, np.y);
+        const float len = GM_FSQRT(GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy)));
+        if (len > p.arrive)
+            p.step_pos[i] = t;
+        else
+            p.state[i] = GMAPF_AGENT_IDLE;
+    } else {
+        const int nd = path[si];
+        p.step_node[i] = nd;
+        p.step_pos[i] = p.cen[nd];
+    }
+}
+
+inline int blocks_for(int n, int bt) { return (n + bt - 1) / bt; }
+
+}  // namespace
+
+void launch_compact(cudaStream_t s, int A, int* state, const int* cur, const int* targ, int P,
+                    int4* req, int* req_count, unsigned char* in_move, int* mv_count, int* work_ctr,
+                    unsigned long long* stats) {
+    k_compact<<<1, kCompactThreads, 0, s>>>(A, state, cur, targ, P, req, req_count, in_move, mv_count,
+                                            work_ctr, stats);
+}
+
+void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, int* targ_node,
+                          float2* targ_pos) {
+    if (n <= 0) return;
+    k_apply_targets<<<blocks_for(n, 256), 256, 0, s>>>(recs, n, state, targ_node, targ_pos);
+}
+
+void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets, int n, int nodes,
+                          int4* req, int* req_count, int* work_ctr, int* err) {
+    k_prepare_batch<<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(starts, targets, n, nodes, req,
+                                                                   req_count, work_ctr, err);
+}
+
+void launch_move_bin(cudaStream_t s, const MoverParams& p) {
+    k_move_bin<<<blocks_for(p.A, 256), 256, 0, s>>>(p);
+}
+
+void launch_cell_scan(cudaStream_t s, const MoverParams& p) { k_cell_scan<<<1, 1024, 0, s>>>(p); }
+
+void launch_scatter(cudaStream_t s, const MoverParams& p) {
+    k_scatter<<<blocks_for(p.A, 256), 256, 0, s>>>(p);
+}
+
+void launch_collide_progress(cudaStream_t s, const MoverParams& p) {
+    k_collide_progress<<<blocks_for(p.A, 128), 128, 0, s>>>(p);
+}
+
+}  // namespace gmapf_b200

@@ -1,0 +1,199 @@
+/*
+ * gmapf_c.h -- C ABI of the B200-native G-MAPF per-frame step.
+ *
+ * The reference (rosdvp/gmapf) exposes only the C++ class gmapf::GMAPF
+ * (include/gmapf/GMAPF.h:30-98) and has no C ABI.  Each entry point below
+ * replaces one member of that class; the citation names the member it
+ * stands for.  include/gmapf/GMAPF.h in this repository is the header-only
+ * C++ wrapper over these functions with the reference's class, method and
+ * type names.
+ *
+ * Conventions: every function returns a gmapf_status (GMAPF_OK == 0);
+ * gmapf_last_error() returns a message for the last failure on the calling
+ * thread.  Plain pointers and sizes only; no C++ or torch types cross.
+ */
+#ifndef GMAPF_C_H
+#define GMAPF_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gmapf_status {
+    GMAPF_OK = 0,
+    GMAPF_E_STATE = 1,          /* lifecycle rule broken (not initialised, already started, ...) */
+    GMAPF_E_INVALID_POS = 2,    /* a position lies in no navmesh triangle */
+    GMAPF_E_CUDA = 3,           /* a CUDA runtime call failed */
+    GMAPF_E_CAPACITY = 4,       /* a fixed capacity would be exceeded */
+    GMAPF_E_DEVICE_TIMEOUT = 5, /* a device-side wait ran out of iterations */
+    GMAPF_E_INVALID_ARG = 6,    /* bad argument (null pointer, out-of-range id or parameter) */
+    GMAPF_E_UNSUPPORTED = 7,    /* feature not compiled in (e.g. the CDT navmesh builder) */
+    GMAPF_E_DEVICE = 8          /* a device-side check failed (bounds / consistency) */
+} gmapf_status;
+
+typedef enum gmapf_agent_state { /* include/gmapf/Agent.h:7-12 (EAgentState) */
+    GMAPF_AGENT_IDLE = 0,
+    GMAPF_AGENT_SEARCH = 1,
+    GMAPF_AGENT_MOVE = 2
+} gmapf_agent_state;
+
+/* include/gmapf/Config.h:5-18 -- same field order, types and layout
+ * (7 x 4-byte fields then two bools; 32 bytes with padding). */
+typedef struct gmapf_config {
+    int32_t AgentsMaxCount;
+    float AgentRadius;
+    float AgentSpeed;
+    int32_t PathFinderParallelAgents;
+    int32_t PathFinderThreadsPerAgents;
+    int32_t PathFinderQueueCapacity;
+    float PathFinderHeuristicK;
+    uint8_t IsDebug;
+    uint8_t IsProfiler;
+} gmapf_config;
+
+/* include/gmapf/misc/V2Float.h:12-16 */
+typedef struct gmapf_v2 {
+    float X;
+    float Y;
+} gmapf_v2;
+
+/* include/gmapf/misc/CuNodesMap.h:14-21 (CuNodesMap::Node, 48 bytes,
+ * 16-byte aligned): three vertices, the centroid (overwritten on ingest),
+ * up to three neighbour ids packed first and padded with -1. */
+typedef struct gmapf_node {
+    gmapf_v2 P1;
+    gmapf_v2 P2;
+    gmapf_v2 P3;
+    gmapf_v2 PCenter;
+    int32_t NeibsIdx[3];
+    int32_t _pad;
+} gmapf_node;
+
+/* Step forms.  Both run the same per-query arithmetic and give identical
+ * results for the same (threads per agent, queue capacity). */
+typedef enum gmapf_mode {
+    GMAPF_MODE_BATCHED = 0, /* persistent search over a device work queue; step replayed as a CUDA graph */
+    GMAPF_MODE_PLAIN = 1    /* one lane group per request in fixed launches; host reads counts back */
+} gmapf_mode;
+
+/* Tuning knobs that are not part of the reference Config. */
+typedef struct gmapf_options {
+    int32_t device;            /* CUDA device ordinal (default 0) */
+    int32_t mode;              /* gmapf_mode (default GMAPF_MODE_BATCHED) */
+    int32_t block_threads;     /* search block size, 0 = automatic */
+    int32_t autotune;          /* 1: pick threads/agent, queue capacity and block size per map at start */
+    int64_t search_mem_budget; /* bytes for per-slot search records, 0 = automatic */
+    int32_t order_by_estimate; /* 1: serve long searches first (results do not depend on it) */
+    int32_t _reserved[5];
+} gmapf_options;
+
+typedef struct gmapf_step_stats {
+    int64_t requests;       /* path requests served this frame */
+    int64_t found;          /* of which found */
+    int64_t expansions;     /* nodes expanded */
+    int64_t rounds;         /* search rounds summed over requests */
+    int64_t deg_sum;        /* sum of the degrees of expanded nodes */
+    int64_t claims;         /* nodes claimed */
+    int64_t path_nodes;     /* sum of path lengths written */
+    int64_t moving;         /* agents in Move at the start of the frame */
+    float ms_step_wall;     /* host wall time AsyncStep -> WaitStepEnd */
+    float ms_search;        /* device time of the search kernel(s) */
+    float ms_mover;         /* device time of the mover kernels */
+    float ms_total_device;  /* device time of the whole frame */
+} gmapf_step_stats;
+
+typedef struct gmapf_ctx gmapf_ctx;
+
+/* Lifecycle (GMAPF.h:32-37 constructor/destructor) */
+gmapf_status gmapf_create(gmapf_ctx** out);
+gmapf_status gmapf_destroy(gmapf_ctx* ctx);
+const char* gmapf_last_error(void);
+
+/* GMAPF::Init(const Config&)            -- src/GMAPF.cu:58-70 */
+gmapf_status gmapf_init(gmapf_ctx* ctx, const gmapf_config* config);
+/* tuning knobs; call between gmapf_init and the start */
+gmapf_status gmapf_set_options(gmapf_ctx* ctx, const gmapf_options* opts);
+gmapf_status gmapf_get_options(gmapf_ctx* ctx, gmapf_options* out);
+
+/* GMAPF::FillMapStart(const V2Float&)   -- src/GMAPF.cu:133-145 */
+gmapf_status gmapf_fill_map_start(gmapf_ctx* ctx, float size_x, float size_y);
+/* GMAPF::FillMapObstacle(vector<V2Float>) -- src/GMAPF.cu:147-159 */
+gmapf_status gmapf_fill_map_obstacle(gmapf_ctx* ctx, const gmapf_v2* vertices, int32_t count);
+/* GMAPF::FillMapEnd()                    -- src/GMAPF.cu:161-196 */
+gmapf_status gmapf_fill_map_end(gmapf_ctx* ctx);
+/* GMAPF::FillMapManually(vector<Node>)   -- src/GMAPF.cu:199-217 */
+gmapf_status gmapf_fill_map_manually(gmapf_ctx* ctx, const gmapf_node* nodes, int32_t count);
+
+/* GMAPF::AddAgent(const V2Float&)        -- src/GMAPF.cu:219-236 */
+gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id);
+/* GMAPF::SetAgentTargPos(int, V2Float)   -- src/GMAPF.cu:238-253
+ * (README.md:78 spells it SetAgentTargetPos; both C++ spellings map here) */
+gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t agent_id, float x, float y);
+/* bulk form of the above: n targets, one call */
+gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* pos, int32_t n);
+
+/* GMAPF::ManualStart()                   -- src/GMAPF.cu:72-130 */
+gmapf_status gmapf_manual_start(gmapf_ctx* ctx);
+/* GMAPF::AsyncStep(float)                -- src/GMAPF.cu:255-289 */
+gmapf_status gmapf_async_step(gmapf_ctx* ctx, float delta_time);
+/* GMAPF::WaitStepEnd()                   -- src/GMAPF.cu:291-314 */
+gmapf_status gmapf_wait_step_end(gmapf_ctx* ctx);
+
+/* GMAPF::GetAgentPos(int)                -- src/GMAPF.cu:316-319 */
+gmapf_status gmapf_get_agent_pos(gmapf_ctx* ctx, int32_t agent_id, gmapf_v2* out);
+/* GMAPF::GetAgentState(int)              -- src/GMAPF.cu:321-324 */
+gmapf_status gmapf_get_agent_state(gmapf_ctx* ctx, int32_t agent_id, int32_t* out);
+/* pointer to the host mirror of all positions (valid until gmapf_destroy;
+ * refreshed by gmapf_wait_step_end); backs GMAPF::GetAgentPos's reference */
+const gmapf_v2* gmapf_agent_pos_view(gmapf_ctx* ctx);
+/* bulk copies of the host mirror */
+gmapf_status gmapf_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* state, int32_t n);
+int32_t gmapf_agent_count(gmapf_ctx* ctx);
+
+/* GMAPF::ProfilerDump()                  -- src/GMAPF.cu:326-356 */
+gmapf_status gmapf_profiler_dump(gmapf_ctx* ctx);
+
+/* ---- inspection (tests, benchmarks, tools); not in the reference API ---- */
+int32_t gmapf_map_count(gmapf_ctx* ctx);
+gmapf_status gmapf_get_map_nodes(gmapf_ctx* ctx, gmapf_node* out, int32_t cap);
+/* host point location with CuNodesMap::TryGetNodeIdx semantics (first
+ * triangle in index order), grid-accelerated; -1 when outside */
+gmapf_status gmapf_locate_points(gmapf_ctx* ctx, const gmapf_v2* pts, int32_t n, int32_t* out_node);
+/* full device agent state, downloaded synchronously (no step may be running) */
+gmapf_status gmapf_debug_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* state, int32_t* cur_node,
+                                    int32_t* targ_node, int32_t* step_idx, int32_t* step_node,
+                                    gmapf_v2* step_pos, int32_t* path_len);
+/* path of one agent (device download); returns its length in *out_len */
+gmapf_status gmapf_debug_get_path(gmapf_ctx* ctx, int32_t agent_id, int32_t* out, int32_t cap, int32_t* out_len);
+/* statistics of the last completed step */
+gmapf_status gmapf_last_step_stats(gmapf_ctx* ctx, gmapf_step_stats* out);
+/* wall-time percentiles (ms) over the recorded steps; q in [0,100] */
+gmapf_status gmapf_step_time_percentile(gmapf_ctx* ctx, float q, float* out_ms);
+gmapf_status gmapf_reset_profiler(gmapf_ctx* ctx);
+/* number of kernel launches issued by the library since creation */
+int64_t gmapf_kernel_launches(gmapf_ctx* ctx);
+
+/* ---- batched query API: searches only, no agents ---- */
+/* Run n independent searches (start/target node ids) with the context's
+ * map and search parameters; writes found flags, lengths and paths
+ * (path i at paths[i * path_stride]).  Inputs and outputs are host
+ * buffers; copies are inside the call. */
+gmapf_status gmapf_search_batch_host(gmapf_ctx* ctx, const int32_t* starts, const int32_t* targets,
+                                     int32_t n, int32_t* found, int32_t* lens, int32_t* paths,
+                                     int32_t path_stride, gmapf_step_stats* stats);
+/* Same with device pointers already resident in HBM (no copies); ordered
+ * on the context's stream; synchronous. */
+gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, const int32_t* d_targets,
+                                       int32_t n, int32_t* d_found, int32_t* d_lens, int32_t* d_paths,
+                                       int32_t path_stride, gmapf_step_stats* stats);
+/* device time (ms) of the last batch search kernel, measured with CUDA
+ * events on the launching stream */
+gmapf_status gmapf_last_search_ms(gmapf_ctx* ctx, float* out_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GMAPF_C_H */

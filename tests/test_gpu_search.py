@@ -1,0 +1,117 @@
+"""Search parity: the CUDA search (through the C ABI) against the oracle, bit-exact
+on found flags, path lengths, triangle sequences and search counters."""
+import numpy as np
+import pytest
+
+import gmapf_b200 as G
+from gmapf_b200 import scenarios as S
+from gpu_util import map_world, random_queries
+
+pytestmark = pytest.mark.gpu
+
+
+def check_batch(oracle_mod, g, starts, targets, T, Cap, K=1.0):
+    nodes = g.map_nodes()
+    om = oracle_mod.OMap(nodes)
+    stride = max(1, om.n)
+    f, l, p, st = g.search_batch(starts, targets, stride)
+    of, ol, op, ost = om.search_batch(starts, targets, T, Cap, K, path_stride=stride)
+    assert np.array_equal(f, of), "found flags differ"
+    assert np.array_equal(l, ol), "path lengths differ"
+    for i in range(len(starts)):
+        if f[i]:
+            assert np.array_equal(p[i, :l[i]], op[i, :ol[i]]), f"path {i} differs"
+    assert st["expansions"] == ost["expansions"]
+    assert st["rounds"] == ost["rounds"]
+    assert st["claims"] == ost["claims"]
+    assert st["deg_sum"] == ost["deg_sum"]
+    return f, l, p, st
+
+
+@pytest.mark.parametrize("T,Cap", [(2, 1), (2, 16), (4, 16), (8, 2), (32, 64)])
+def test_cfg1_all_pairs(oracle_mod, T, Cap):
+    scn = S.cfg1()
+    g = map_world(scn, T=T, Cap=Cap)
+    n = g.node_count
+    s, t = np.meshgrid(np.arange(n), np.arange(n))
+    f, l, p, st = check_batch(oracle_mod, g, s.ravel().astype(np.int32), t.ravel().astype(np.int32), T, Cap)
+    assert f.mean() > 0.5
+
+
+@pytest.mark.parametrize("T,Cap", [(8, 32), (4, 16), (16, 8)])
+def test_cfg2_random(oracle_mod, T, Cap):
+    scn = S.cfg2()
+    g = map_world(scn, T=T, Cap=Cap)
+    s, t = random_queries(g, scn, 2048, seed=11)
+    check_batch(oracle_mod, g, s, t, T, Cap)
+
+
+@pytest.mark.parametrize("T,Cap", [(8, 32), (32, 64), (2, 256)])
+def test_maze64_random(oracle_mod, T, Cap):
+    scn = S.cfg3(cells=64)
+    g = map_world(scn, T=T, Cap=Cap)
+    s, t = random_queries(g, scn, 512, seed=12)
+    f, l, p, st = check_batch(oracle_mod, g, s, t, T, Cap)
+    # path validity: consecutive triangles are neighbours and the path ends at the target
+    nb = g.map_nodes()["NeibsIdx"]
+    for i in range(len(s)):
+        if f[i] and l[i] > 0:
+            seq = [s[i]] + list(p[i, :l[i]])
+            assert seq[-1] == t[i]
+            for a, b in zip(seq[:-1], seq[1:]):
+                assert b in nb[a]
+
+
+def test_plain_equals_batched(oracle_mod):
+    scn = S.cfg2()
+    gb = map_world(scn, T=8, Cap=32, mode=G.MODE_BATCHED)
+    gp = map_world(scn, T=8, Cap=32, mode=G.MODE_PLAIN)
+    s, t = random_queries(gb, scn, 1500, seed=13)
+    fb, lb, pb, _ = gb.search_batch(s, t, gb.node_count)
+    fp, lp, pp, _ = gp.search_batch(s, t, gp.node_count)
+    assert np.array_equal(fb, fp) and np.array_equal(lb, lp) and np.array_equal(pb, pp)
+
+
+@pytest.mark.parametrize("bt", [32, 64, 256])
+def test_block_shape_does_not_change_results(oracle_mod, bt):
+    scn = S.cfg2()
+    g = map_world(scn, T=4, Cap=16, block_threads=bt)
+    s, t = random_queries(g, scn, 700, seed=14)
+    check_batch(oracle_mod, g, s, t, 4, 16)
+
+
+def test_edge_cases(oracle_mod):
+    scn = S.cfg1()
+    g = map_world(scn, T=4, Cap=16)
+    n = g.node_count
+    # empty batch
+    f, l, p, st = g.search_batch(np.zeros(0, np.int32), np.zeros(0, np.int32), n)
+    assert len(f) == 0
+    # start == target: found, empty path
+    f, l, p, st = g.search_batch(np.array([3], np.int32), np.array([3], np.int32), n)
+    assert f[0] == 1 and l[0] == 0
+    # out-of-range node ids are rejected on the host
+    with pytest.raises(G.GMAPFError) as e:
+        g.search_batch(np.array([n], np.int32), np.array([0], np.int32), n)
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
+    # the same batch twice gives the same answer (slot epochs, no clearing)
+    s = np.arange(n, dtype=np.int32)
+    t = s[::-1].copy()
+    a = g.search_batch(s, t, n)
+    b = g.search_batch(s, t, n)
+    assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
+
+
+def test_disconnected_map_not_found(oracle_mod):
+    # two separate triangles: searches between them exhaust both queues
+    g = G.GMAPF()
+    g.Init(G.make_config(4, 1, 1, 4, 4, 16))
+    nodes = np.zeros(4, G.NODE_DTYPE)
+    nodes["P1"] = [[0, 0], [1, 0], [10, 0], [11, 0]]
+    nodes["P2"] = [[1, 0], [1, 1], [11, 0], [11, 1]]
+    nodes["P3"] = [[0, 1], [0, 1], [10, 1], [10, 1]]
+    nodes["NeibsIdx"] = [[1, -1, -1], [0, -1, -1], [3, -1, -1], [2, -1, -1]]
+    g.FillMapManually(nodes)
+    f, l, p, st = g.search_batch(np.array([0, 0, 2], np.int32), np.array([3, 1, 3], np.int32), 4)
+    assert f.tolist() == [0, 1, 1]
+    assert l.tolist() == [0, 1, 1]

@@ -1,0 +1,108 @@
+"""Full per-frame step parity: AsyncStep/WaitStepEnd through the C ABI against
+the oracle world; paths and states exact, positions within 1e-4 relative."""
+import numpy as np
+import pytest
+
+import gmapf_b200 as G
+from gmapf_b200 import scenarios as S
+from gpu_util import close_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None):
+    g, starts, rng = S.make_world(scn, mode=mode, agents=agents, threads_per_agent=T, queue_capacity=Cap,
+                                  parallel_agents=P)
+    om = oracle_mod.OMap(g.map_nodes())
+    ow = oracle_mod.OWorld(om, agents, scn.radius, scn.speed, P or agents, T or scn.threads_per_agent,
+                           Cap or scn.queue_capacity, scn.heuristic_k)
+    for p in starts:
+        assert ow.add_agent(p[0], p[1]) >= 0
+    return g, ow, rng
+
+
+def retarget(g, ow, scn, ids, rng):
+    tp = S.free_points(g, scn, len(ids), rng)
+    g.set_targets(ids, tp)
+    for i, p in zip(ids, tp):
+        assert ow.set_target(int(i), p[0], p[1]) == 0
+
+
+def compare(g, ow, step):
+    d = g.debug_agents()
+    o = ow.get()
+    for k in ["state", "cur_node", "targ_node", "step_idx", "step_node", "path_len"]:
+        assert np.array_equal(d[k], o[k]), f"{k} differs at step {step}"
+    ok, mx = close_rel(d["pos"], o["pos"])
+    assert ok, f"positions differ at step {step} (max abs diff {mx})"
+    ok, mx = close_rel(d["step_pos"], o["step_pos"])
+    assert ok, f"step targets differ at step {step}"
+    return d
+
+
+def run(g, ow, scn, steps, rng, retarget_every=0, check_every=10, threads=8):
+    A = g.agent_count
+    for k in range(steps):
+        if retarget_every and k % retarget_every == 0:
+            retarget(g, ow, scn, np.arange(A), rng)
+        g.AsyncStep(scn.dt)
+        g.WaitStepEnd()
+        ow.step(scn.dt, threads)
+        if (k + 1) % check_every == 0 or k == steps - 1:
+            d = compare(g, ow, k)
+    return d
+
+
+def test_cfg1_200_steps(oracle_mod):
+    scn = S.cfg1()
+    g, ow, rng = make_pair(oracle_mod, scn, scn.agents)
+    retarget(g, ow, scn, np.arange(scn.agents), rng)
+    d = run(g, ow, scn, 200, rng)
+    # paths identical for every agent that has one
+    for i in range(scn.agents):
+        if d["path_len"][i] > 0:
+            assert np.array_equal(g.path(i), ow.path(i))
+    # host mirror equals the device state after WaitStepEnd
+    pos, st = g.agents()
+    assert np.array_equal(st, d["state"])
+    assert np.array_equal(pos, d["pos"], equal_nan=True)
+
+
+def test_cfg2_retargets(oracle_mod):
+    scn = S.cfg2()
+    g, ow, rng = make_pair(oracle_mod, scn, 512)
+    run(g, ow, scn, 250, rng, retarget_every=100, check_every=25)
+
+
+def test_plain_mode_step(oracle_mod):
+    scn = S.cfg1()
+    g, ow, rng = make_pair(oracle_mod, scn, 128, mode=G.MODE_PLAIN)
+    retarget(g, ow, scn, np.arange(128), rng)
+    run(g, ow, scn, 120, rng, check_every=30)
+
+
+def test_request_capacity_defers(oracle_mod):
+    # PathFinderParallelAgents below the number of searching agents: the rest
+    # stay in Search for later frames (PathFinder.h:97-102)
+    scn = S.cfg1()
+    g, ow, rng = make_pair(oracle_mod, scn, 200, P=64)
+    retarget(g, ow, scn, np.arange(200), rng)
+    g.AsyncStep(scn.dt)
+    g.WaitStepEnd()
+    ow.step(scn.dt)
+    st = g.last_stats()
+    assert st["requests"] == 64
+    compare(g, ow, 0)
+    run(g, ow, scn, 30, rng, check_every=5)
+
+
+def test_zigzag_reference_driver(oracle_mod):
+    # main.cpp TestFull layout: agents at (i/5, 0) heading to (i/5, 950)
+    scn = S.zigzag()
+    A = 1024
+    g, ow, rng = make_pair(oracle_mod, scn, A, T=2, Cap=16)
+    tp = np.array([[i / 5.0, 950.0] for i in range(A)], np.float32)
+    g.set_targets(np.arange(A), tp)
+    for i, p in enumerate(tp):
+        ow.set_target(i, p[0], p[1])
+    run(g, ow, scn, 60, rng, check_every=20)
