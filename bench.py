@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""bench.py -- the G-MAPF per-frame step on B200.
+
+Workload (one "step" = one frame with every agent retargeted, the
+batched-uneven-queries configuration): a 4000x4000 maze built by seeded
+randomized DFS over cells x cells (walls 4 wide) and triangulated by CDT on
+the host, 16,384 agents of radius 2 and speed 1, every agent given a fresh
+uniform free-space target before each frame, threads/agent T and queue
+capacity C.  One frame = request compaction, the searches (path queries),
+path writes, mover (move, grid collisions, path progress) and the copy of
+positions and states back to the host mirror.
+
+  value  path queries/s with the targets already resident in device memory
+         (device-side retarget + frame, CUDA events on the library's stream,
+         summed over the timed frames; L2 flushed between frames)
+  e2e    the same through the reference-facing API with host buffers:
+         SetAgentTargPos (bulk) -> AsyncStep -> WaitStepEnd, host wall time
+  plain  the plain per-agent form (one static launch per request chunk, host
+         read-back of counts), same arithmetic, same frames
+
+`--impl reference` times the reference's own CPU implementation of the path:
+the reference has none, so it is the C++ restatement in oracle/ (the
+deterministic port of the reference's step), multithreaded over all host
+cores, on a bounded sample of each frame's requests.
+
+Multi-GPU (torchrun): every rank runs its own scene (weak scaling, no data
+path collective); the timed region is bracketed by a barrier and the time
+is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "p99 step ms & path queries/s at 16k agents, batched vs plain, on 1 B200"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------- helpers --
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return ws, rank, local
+
+
+def init_dist(ws, local, use_cuda=True):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    backend = "nccl" if use_cuda and torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def reduce_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(st: dict, n_nodes: int) -> float:
+    """Search bytes by the fixed per-unit definitions: per expansion 12 B of
+    adjacency plus 24 B per neighbour (centroid, visited word, record); per
+    query N/4 B of visited bitmap, 16 B of request and 4 B per path node."""
+    return (12.0 * st["expansions"] + 24.0 * st["deg_sum"] + st["requests"] * (n_nodes / 4.0 + 16.0)
+            + 4.0 * st["path_nodes"])
+
+
+# --------------------------------------------------------------- b200 arm --
+
+def make_scene(cells, seed, T, C, mode, agents, profiler=True):
+    from gmapf_b200 import scenarios as S
+    scn = S.cfg3(cells=cells, seed=seed, agents=agents, threads_per_agent=T, queue_capacity=C)
+    g, starts, rng = S.make_world(scn, mode=mode, profiler=profiler)
+    g.ManualStart()
+    return scn, g, rng
+
+
+def target_sets(g, scn, rng, k, A):
+    from gmapf_b200 import scenarios as S
+    return [S.free_points(g, scn, A, rng) for _ in range(k)]
+
+
+def run_frames_device(g, sets, warmup, steps, torch, flush):
+    """value: device-resident retargets; per-frame device time on the library's stream."""
+    A = sets[0].shape[0]
+    dev_ids = torch.arange(A, dtype=torch.int32, device="cuda")
+    dev_sets = [torch.from_numpy(s).cuda() for s in sets]
+    ext = torch.cuda.ExternalStream(g.stream_handle)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    stats, ms = [], []
+    launches0 = None
+    for k in range(warmup + steps):
+        flush.zero_()  # L2 flush (larger than the 126 MB L2), outside the timed window
+        torch.cuda.synchronize()
+        if k == warmup:
+            launches0 = g.kernel_launches
+        tk = k - warmup
+        if tk >= 0:
+            ev[tk][0].record(ext)
+        g.set_targets_device(dev_ids.data_ptr(), dev_sets[k].data_ptr(), A)
+        g.AsyncStep(1.0 / 60.0)
+        if tk >= 0:
+            ev[tk][1].record(ext)
+        g.WaitStepEnd()
+        if tk >= 0:
+            stats.append(g.last_stats())
+    torch.cuda.synchronize()
+    launches = g.kernel_launches - launches0
+    ms = [a.elapsed_time(b) for a, b in ev]
+    return ms, stats, launches
+
+
+def run_frames_host(g, sets, warmup, steps):
+    """e2e: host buffers through the reference-facing API."""
+    A = sets[0].shape[0]
+    ids = np.arange(A, dtype=np.int32)
+    wall, stats = [], []
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        g.set_targets(ids, sets[k])
+        g.AsyncStep(1.0 / 60.0)
+        g.WaitStepEnd()
+        t1 = time.perf_counter()
+        if k >= warmup:
+            wall.append((t1 - t0) * 1e3)
+            stats.append(g.last_stats())
+    return wall, stats
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q, method="higher")) if len(v) else None
+
+
+def cpu_baseline(g, scn, sets, T, C, sample, threads):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    om = O.OMap(g.map_nodes())
+    d = g.debug_agents()
+    starts = d["cur_node"][:sample]
+    targets = g.locate(sets[0][:sample])
+    t0 = time.perf_counter()
+    found, lens, _, st = om.search_batch(starts, targets, T, C, threads=threads, path_stride=0)
+    dt = time.perf_counter() - t0
+    return {"value": sample / dt, "unit": "path queries/s", "cores": threads, "kind": "port",
+            "sample": f"{sample} of the frame's {len(sets[0])} queries (same map, T={T}, C={C}), "
+                      f"oracle/ C++ restatement, {threads} host threads"}
+
+
+def bench_b200(args):
+    import torch
+    ws, rank, local = dist_env()
+    dist = init_dist(ws, local)
+    torch.cuda.set_device(local)
+    import gmapf_b200 as G
+
+    A = args.agents
+    T, C = args.threads_per_agent, args.queue_capacity
+    seed = 3 + rank
+    scn, g, rng = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A)
+    n_nodes = g.node_count
+    shape = g.search_shape()
+    K, W = args.steps, args.warmup
+    sets = target_sets(g, scn, rng, W + K, A)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    barrier(dist)
+    with ClockSampler(local) as clk:
+        ms, dstats, launches = run_frames_device(g, sets, W, K, torch, flush)
+    barrier(dist)
+    dev_total_ms = reduce_max(dist, float(sum(ms)))
+    queries = float(sum(s["requests"] for s in dstats))
+    all_queries = reduce_sum(dist, queries)
+    value = all_queries / (dev_total_ms / 1e3)
+
+    # e2e through the host API (fresh targets, same scene)
+    sets_e2e = target_sets(g, scn, rng, W + K, A)
+    g.reset_profiler()
+    barrier(dist)
+    wall, hstats = run_frames_host(g, sets_e2e, W, K)
+    barrier(dist)
+    e2e_total = reduce_max(dist, float(sum(wall)))
+    e2e_q = reduce_sum(dist, float(sum(s["requests"] for s in hstats)))
+    e2e_value = e2e_q / (e2e_total / 1e3)
+
+    # roofline of the dominant kernel (search), from the profiler's CUDA events
+    search_ms = [s["ms_search"] for s in dstats]
+    ab = [algorithmic_bytes(s, n_nodes) for s in dstats]
+    achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # plain per-agent form on the same frames
+    plain = None
+    if not args.no_plain:
+        scn_p, gp, rng_p = make_scene(args.cells, seed, T, C, G.MODE_PLAIN, A)
+        pk = max(2, min(K, 5))
+        wall_p, pst = run_frames_host(gp, sets[:1 + pk], 1, pk)
+        plain = {"value": sum(s["requests"] for s in pst) / (sum(wall_p) / 1e3), "unit": "path queries/s",
+                 "p99_step_ms": pct(wall_p, 99), "ms_per_step": statistics.mean(wall_p), "steps": pk}
+        gp.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(g, scn, sets, T, C, args.cpu_sample, os.cpu_count() or 1)
+
+    # secondary workload: the 64x64-cell maze of the configuration text
+    secondary = None
+    if args.secondary_cells and args.secondary_cells != args.cells and rank == 0:
+        scn2, g2, rng2 = make_scene(args.secondary_cells, 3, T, C, G.MODE_BATCHED, A)
+        sets2 = target_sets(g2, scn2, rng2, W + K, A)
+        ms2, st2, _ = run_frames_device(g2, sets2, W, K, torch, flush)
+        wall2, _ = run_frames_host(g2, target_sets(g2, scn2, rng2, W + K, A), W, K)
+        secondary = {"workload": f"maze {args.secondary_cells}x{args.secondary_cells} cells",
+                     "triangles": g2.node_count,
+                     "value": sum(s["requests"] for s in st2) / (sum(ms2) / 1e3),
+                     "e2e_value": A * K / (sum(wall2) / 1e3), "p99_step_ms": pct(wall2, 99),
+                     "p50_step_ms": pct(wall2, 50), "ms_per_step_device": statistics.mean(ms2)}
+        g2.close()
+
+    if rank == 0:
+        st_sum = {k: sum(s[k] for s in dstats) for k in ["requests", "found", "expansions", "rounds", "claims"]}
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "path queries/s",
+            "n_gpus": ws,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": dev_total_ms / K,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+i32",
+            "data": "synthetic: seeded randomized-DFS maze, uniform free-space starts and targets",
+            "config": {"workload": f"maze {args.cells}x{args.cells} cells on 4000x4000, {A} agents, all "
+                                   f"retargeted every frame", "triangles": n_nodes, "agents": A,
+                       "threads_per_agent": T, "queue_capacity": C, "block_threads": shape["block_threads"],
+                       "visited_mode": "shared-memory bitmap" if shape["visited_mode"] == 1 else "global records",
+                       "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",
+                       "l2": "flushed between frames (256 MB write); per-frame search records exceed L2",
+                       "parallelism": f"{ws} independent scenes (one per GPU)"},
+            "p99_step_ms": pct(wall, 99),
+            "p50_step_ms": pct(wall, 50),
+            "device_ms_per_step": {"mean": statistics.mean(ms), "p99": pct(ms, 99), "max": max(ms)},
+            "found_rate": st_sum["found"] / max(1, st_sum["requests"]),
+            "expansions_per_s": st_sum["expansions"] / (sum(ms) / 1e3),
+            "plain": plain,
+            "batched_over_plain": (e2e_value / plain["value"]) if plain else None,
+            "roofline": {"bound": "hbm", "kernel": "k_search", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "search_ms_per_step": statistics.mean(search_ms),
+                         "algorithmic_bytes_per_step": statistics.mean(ab)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "path queries/s", "h2d_bytes_per_step": 16 * A + 4,
+                    "d2h_bytes_per_step": 12 * A + 64 + 8 * 8, "p99_step_ms": pct(wall, 99),
+                    "p50_step_ms": pct(wall, 50)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "secondary": secondary,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------- reference arm --
+
+def bench_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    import gmapf_b200 as G
+    from gmapf_b200 import scenarios as S
+    T, C, A = args.threads_per_agent, args.queue_capacity, args.agents
+    scn = S.cfg3(cells=args.cells, seed=3, agents=A, threads_per_agent=T, queue_capacity=C)
+    g = G.GMAPF()
+    g.Init(G.make_config(4, scn.radius, scn.speed, 4, T, C))
+    S.build_map(g, scn)
+    om = O.OMap(g.map_nodes())
+    rng = np.random.default_rng(1003)
+    threads = os.cpu_count() or 1
+    sample = args.ref_sample
+    times, qs = [], []
+    for k in range(args.warmup + args.steps):
+        s = g.locate(S.free_points(g, scn, sample, rng))
+        t = g.locate(S.free_points(g, scn, sample, rng))
+        t0 = time.perf_counter()
+        om.search_batch(s, t, T, C, threads=threads, path_stride=0)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+            qs.append(sample)
+    value = sum(qs) / sum(times)
+    desc = (f"{sample} queries per step of the {A}-agent frame (uniform free-space starts/targets, same maze, "
+            f"T={T}, C={C}); the reference has no CPU step, so this is its C++ restatement in oracle/")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path queries/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i32",
+            "data": "synthetic: seeded randomized-DFS maze, uniform free-space starts and targets",
+            "config": {"workload": f"maze {args.cells}x{args.cells} cells on 4000x4000, {A} agents, all "
+                                   f"retargeted every frame", "triangles": g.node_count,
+                       "threads_per_agent": T, "queue_capacity": C, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "path queries/s", "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "path queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=160, help="maze cells per side (160: ~100k triangles)")
+    ap.add_argument("--secondary-cells", type=int, default=64, help="also report this maze (0: off)")
+    ap.add_argument("--agents", type=int, default=16384)
+    ap.add_argument("--threads-per-agent", type=int, default=8)
+    ap.add_argument("--queue-capacity", type=int, default=32)
+    ap.add_argument("--cpu-sample", type=int, default=2048)
+    ap.add_argument("--ref-sample", type=int, default=2048)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warmup raised to 3 (timing rule)")
+        args.warmup = 3
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_b200(args)
+
+
+if __name__ == "__main__":
+    main()

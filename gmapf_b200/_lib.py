@@ -49,7 +49,8 @@ class Options(C.Structure):
         ("autotune", C.c_int32),
         ("search_mem_budget", C.c_int64),
         ("order_by_estimate", C.c_int32),
-        ("_reserved", C.c_int32 * 5),
+        ("visited_mode", C.c_int32),
+        ("_reserved", C.c_int32 * 4),
     ]
 
 
@@ -93,6 +94,7 @@ SIGNATURES = {
     "gmapf_add_agent": (C.c_int, [P, C.c_float, C.c_float, I32P]),
     "gmapf_set_agent_targ_pos": (C.c_int, [P, C.c_int32, C.c_float, C.c_float]),
     "gmapf_set_agent_targ_pos_bulk": (C.c_int, [P, I32P, V2P, C.c_int32]),
+    "gmapf_set_agent_targ_pos_device": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int32]),
     "gmapf_manual_start": (C.c_int, [P]),
     "gmapf_async_step": (C.c_int, [P, C.c_float]),
     "gmapf_wait_step_end": (C.c_int, [P]),
@@ -111,6 +113,8 @@ SIGNATURES = {
     "gmapf_step_time_percentile": (C.c_int, [P, C.c_float, C.POINTER(C.c_float)]),
     "gmapf_reset_profiler": (C.c_int, [P]),
     "gmapf_kernel_launches": (C.c_int64, [P]),
+    "gmapf_search_shape": (C.c_int, [P, I32P, I32P, I32P, I32P, I32P]),
+    "gmapf_stream_handle": (C.c_void_p, [P]),
     "gmapf_search_batch_host": (C.c_int, [P, I32P, I32P, C.c_int32, I32P, I32P, I32P, C.c_int32,
                                           C.POINTER(StepStats)]),
     "gmapf_search_batch_device": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,

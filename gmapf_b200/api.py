@@ -144,7 +144,8 @@ class GMAPF:
 
     # -- extras ------------------------------------------------------------
     def set_options(self, mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0,
-                    autotune: bool = False, search_mem_budget: int = 0, order_by_estimate: bool = False) -> None:
+                    autotune: bool = False, search_mem_budget: int = 0, order_by_estimate: bool = False,
+                    visited_mode: int = 0) -> None:
         o = Options()
         o.device = device
         o.mode = mode
@@ -152,6 +153,7 @@ class GMAPF:
         o.autotune = 1 if autotune else 0
         o.search_mem_budget = search_mem_budget
         o.order_by_estimate = 1 if order_by_estimate else 0
+        o.visited_mode = visited_mode
         self._check(self._lib.gmapf_set_options(self._h, C.byref(o)))
 
     def options(self) -> dict:
@@ -184,6 +186,11 @@ class GMAPF:
         p = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 2)
         self._check(self._lib.gmapf_set_agent_targ_pos_bulk(self._h, _ptr(ids), p.ctypes.data_as(C.POINTER(V2)),
                                                              len(ids)))
+
+    def set_targets_device(self, d_ids: int, d_pos: int, n: int) -> None:
+        """Retarget n agents from device-resident ids (int32) and positions
+        (float32 pairs); raw device addresses, enqueued before the next step."""
+        self._check(self._lib.gmapf_set_agent_targ_pos_device(self._h, d_ids, d_pos, int(n)))
 
     def agents(self):
         n = self.agent_count
@@ -229,6 +236,16 @@ class GMAPF:
     @property
     def kernel_launches(self) -> int:
         return self._lib.gmapf_kernel_launches(self._h)
+
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t of the library (0 before the start)."""
+        return self._lib.gmapf_stream_handle(self._h) or 0
+
+    def search_shape(self) -> dict:
+        v = [C.c_int32() for _ in range(5)]
+        self._check(self._lib.gmapf_search_shape(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(["T", "C", "block_threads", "visited_mode", "slots"], [x.value for x in v]))
 
     def search_batch(self, starts, targets, path_stride: int):
         """Independent searches on host buffers (copies inside the call)."""

@@ -269,6 +269,20 @@ gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, c
     return GMAPF_OK;
 }
 
+gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_ids, const gmapf_v2* d_pos,
+                                             int32_t n) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.started) return fail(GMAPF_E_STATE, "not started");
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    if (n < 0 || (n > 0 && (!d_ids || !d_pos))) return fail(GMAPF_E_INVALID_ARG, "bad device arrays");
+    if (n == 0) return GMAPF_OK;
+    std::string err;
+    int rc = device_set_targets_device(c, d_ids, d_pos, n, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
 gmapf_status gmapf_manual_start(gmapf_ctx* ctx) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
@@ -433,6 +447,24 @@ gmapf_status gmapf_reset_profiler(gmapf_ctx* ctx) {
 }
 
 int64_t gmapf_kernel_launches(gmapf_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+
+void* gmapf_stream_handle(gmapf_ctx* ctx) {
+    if (!ctx || !ctx->c.started) return nullptr;
+    return (void*)ctx->c.dev.stream;
+}
+
+gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t* bt, int32_t* vm,
+                                int32_t* slots) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!c.started) return fail(GMAPF_E_STATE, "not started");
+    if (T) *T = c.T;
+    if (C) *C = c.C;
+    if (bt) *bt = c.block_threads;
+    if (vm) *vm = c.dev.smemv ? 1 : 2;
+    if (slots) *slots = c.dev.slots;
+    return GMAPF_OK;
+}
 
 gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, const int32_t* d_targets,
                                        int32_t n, int32_t* d_found, int32_t* d_lens, int32_t* d_paths,

@@ -36,7 +36,8 @@ namespace gmapf_b200 {
 
 namespace {
 
-enum Counter { CT_REQ = 0, CT_MOVE = 1, CT_WORK = 2, CT_ERR = 3, CT_COUNT = 16 };
+// device counters: [8] holds the frame's speed*dt as a float
+enum Counter { CT_REQ = 0, CT_MOVE = 1, CT_WORK = 2, CT_ERR = 3, CT_ERR_TARGETS = 4, CT_COUNT = 16 };
 
 template <class T>
 int dalloc(Context& c, T** p, size_t count, std::string& err) {
@@ -152,37 +153,55 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     Device& d = c.dev;
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device));
-    if (c.opt.block_threads == 0) {
-        // largest block (up to 128 threads) whose queues fit in shared memory
-        for (int cand : {128, 64, 32}) {
-            if (cand % c.T) continue;
-            c.block_threads = cand;
-            if (search_max_blocks_per_sm(c.T, c.C, cand) > 0) break;
-        }
-    }
-    const int bt = c.block_threads;
-    int per_sm = search_max_blocks_per_sm(c.T, c.C, bt);
-    if (per_sm <= 0) {
-        err = "search kernel cannot be resident with T=" + std::to_string(c.T) +
-              " C=" + std::to_string(c.C) + " block=" + std::to_string(bt);
-        return GMAPF_E_INVALID_ARG;
-    }
-    const int gpb = bt / c.T;
-    long long occ_slots = (long long)sms * per_sm * gpb;
     size_t freeb = 0, totalb = 0;
     CK(cudaMemGetInfo(&freeb, &totalb));
     long long budget = c.opt.search_mem_budget > 0 ? c.opt.search_mem_budget : (40ll << 30);
     budget = std::min<long long>(budget, (long long)(freeb * 0.6));
     const long long per_slot = (long long)std::max(1, c.map.n) * (long long)sizeof(Rec);
-    long long mem_slots = budget / per_slot;
-    long long slots = std::min(occ_slots, mem_slots);
-    slots = (slots / gpb) * gpb;
-    if (slots < gpb) {
-        err = "not enough device memory for one block of search slots";
+    const long long mem_slots = budget / per_slot;
+    d.bm_words = search_bitmap_words(std::max(1, c.map.n));
+
+    // Candidates: visited state on chip (bitmap) or in global records, and
+    // the block size.  The score is the number of resident lane groups, with
+    // on-chip claims counted double (they remove one L2 round trip from every
+    // round).
+    long long best_score = -1;
+    int best_bt = 0;
+    bool best_smem = false;
+    long long best_slots = 0;
+    for (int vm = 1; vm <= 2; vm++) {
+        if (c.opt.visited_mode != 0 && c.opt.visited_mode != vm) continue;
+        const bool smem = vm == 1;
+        const int bts[4] = {128, 64, 32, 256};
+        for (int bt : bts) {
+            if (c.opt.block_threads != 0 && bt != c.opt.block_threads) continue;
+            if (bt % c.T) continue;
+            const int per_sm = search_max_blocks_per_sm(c.T, c.C, bt, smem, d.bm_words);
+            if (per_sm <= 0) continue;
+            const int gpb = bt / 32;  // one request slot per warp
+            long long slots = std::min((long long)sms * per_sm * gpb, mem_slots);
+            slots = (slots / gpb) * gpb;
+            if (slots < gpb) continue;
+            const long long score = slots * (smem ? 2 : 1);
+            if (score > best_score) {
+                best_score = score;
+                best_bt = bt;
+                best_smem = smem;
+                best_slots = slots;
+            }
+        }
+    }
+    if (best_score < 0) {
+        err = "search kernel cannot be resident with T=" + std::to_string(c.T) + " C=" +
+              std::to_string(c.C) + " (shared memory or device memory too small)";
         return GMAPF_E_CAPACITY;
     }
-    blocks = (int)(slots / gpb);
-    d.slots = (int)slots;
+    c.block_threads = best_bt;
+    d.smemv = best_smem;
+    d.slots = (int)best_slots;
+    blocks = (int)(best_slots / (best_bt / 32));
+    // leave the kernel's shared-memory limit set for the chosen shape
+    search_max_blocks_per_sm(c.T, c.C, best_bt, best_smem, d.bm_words);
     return GMAPF_OK;
 }
 
@@ -210,7 +229,7 @@ void free_search_state(Context& c) {
     d.slots = 0;
 }
 
-int search_blocks(Context& c) { return c.dev.slots / (c.block_threads / c.T); }
+int search_blocks(Context& c) { return c.dev.slots / (c.block_threads / 32); }
 
 void destroy_graph(Context& c) {
     if (c.dev.graph_exec) cudaGraphExecDestroy(c.dev.graph_exec);
@@ -232,7 +251,7 @@ int enqueue_frame(Context& c, bool timing, std::string& err) {
     CK(cudaStreamWaitEvent(s2, d.ev[5], 0));
     // search branch
     SearchParams sp = search_params(c);
-    CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0));
+    CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.smemv, d.bm_words));
     if (timing) CK(cudaEventRecordWithFlags(d.ev[2], s, cudaEventRecordExternal));
     // mover branch
     MoverParams mp = mover_params(c);
@@ -445,9 +464,9 @@ int device_async_step(Context& c, float dt, std::string& err) {
             const int chunk = d.slots;
             for (int base = 0; base < R; base += chunk) {
                 const int cnt = std::min(chunk, R - base);
-                const int gpb = c.block_threads / c.T;
+                const int gpb = c.block_threads / 32;
                 const int blocks = (cnt + gpb - 1) / gpb;
-                CK(launch_search(s, sp, blocks, c.block_threads, false, base));
+                CK(launch_search(s, sp, blocks, c.block_threads, false, base, d.smemv, d.bm_words));
                 c.launches += 1;
             }
         }
@@ -534,10 +553,27 @@ int device_wait_step(Context& c, std::string& err) {
     }
     c.prof.wall_ms.push_back(st.ms_step_wall);
     const int e = c.h_small[CT_ERR];
+    const int et = c.h_small[CT_ERR_TARGETS];
+    if (et != 0) {  // from device-resident retargets enqueued before this step
+        CK(cudaMemset(d.counters + CT_ERR_TARGETS, 0, sizeof(int)));
+        err = "device-resident retarget rejected (agent id out of range or position in no triangle)";
+        return GMAPF_E_DEVICE;
+    }
     if (e != 0) {
         err = "device-side check failed (error bits " + std::to_string(e) + ")";
         return GMAPF_E_DEVICE;
     }
+    return GMAPF_OK;
+}
+
+int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, std::string& err) {
+    Device& d = c.dev;
+    CK(cudaSetDevice(d.device));
+    MoverParams mp = mover_params(c);
+    launch_apply_targets_device(d.stream, d_ids, reinterpret_cast<const float2*>(d_pos), n, c.A, mp.loc, d.state,
+                                d.targ, d.targ_pos, d.counters + CT_ERR_TARGETS);
+    c.launches += 1;
+    CK(cudaGetLastError());
     return GMAPF_OK;
 }
 
@@ -576,14 +612,14 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
     CK(cudaEventRecord(d.ev[6], s));
     if (n > 0) {
         if (c.opt.mode == GMAPF_MODE_BATCHED) {
-            CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0));
+            CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.smemv, d.bm_words));
             c.launches += 1;
         } else {
             sp.req_count_h = n;
-            const int gpb = c.block_threads / c.T;
+            const int gpb = c.block_threads / 32;
             for (int base = 0; base < n; base += d.slots) {
                 const int cnt = std::min(d.slots, n - base);
-                CK(launch_search(s, sp, (cnt + gpb - 1) / gpb, c.block_threads, false, base));
+                CK(launch_search(s, sp, (cnt + gpb - 1) / gpb, c.block_threads, false, base, d.smemv, d.bm_words));
                 c.launches += 1;
             }
         }

@@ -69,8 +69,10 @@ void build_host_map(const gmapf_node* nodes, int n, HostMap& m) {
         r.y1 = c1.y;
         r.x2 = c2.x;
         r.y2 = c2.y;
-        r.cx = m.cen[i].x;
-        r.cy = m.cen[i].y;
+        for (int k = 0; k < 3; k++)
+            for (int j = 0; j < 3; j++)
+                r.g[3 * k + j] = nb[k] >= 0 ? m.nodes[nb[k]].NeibsIdx[j] : -1;
+        r.pad = 0;
         m.rows[i] = r;
     }
 

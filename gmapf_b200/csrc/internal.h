@@ -113,6 +113,9 @@ void launch_compact(cudaStream_t s, int A, int* state, const int* cur, const int
                     unsigned long long* stats);
 void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, int* targ_node,
                           float2* targ_pos);
+void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int A,
+                                 const LocateGrid& loc, int* state, int* targ_node, float2* targ_pos,
+                                 int* err);
 void launch_move_bin(cudaStream_t s, const MoverParams& p);
 void launch_cell_scan(cudaStream_t s, const MoverParams& p);
 void launch_scatter(cudaStream_t s, const MoverParams& p);
@@ -122,10 +125,13 @@ void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets,
 // search.cu
 // persistent: groups pull requests from *work_ctr until *req_count_d is reached.
 // plain: one request per group, requests [base, base + groups).
+// smem_visited: visited bitmap in shared memory (bm_words 32-bit words per
+// lane group) instead of stamped records in global memory.
 cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int block_threads,
-                          bool persistent, int req_base);
-size_t search_smem_bytes(int T, int C, int block_threads);
-int search_max_blocks_per_sm(int T, int C, int block_threads);
+                          bool persistent, int req_base, bool smem_visited, int bm_words);
+size_t search_smem_bytes(int C, int block_threads, int bm_words_per_group, int T);
+int search_bitmap_words(int n_nodes);
+int search_max_blocks_per_sm(int T, int C, int block_threads, bool smem_visited, int bm_words);
 
 // ------------------------------------------------------------------- host --
 
@@ -178,6 +184,8 @@ struct Device {
     Rec* rec = nullptr;
     unsigned* epoch = nullptr;
     int slots = 0;
+    bool smemv = false;  // visited bitmap in shared memory
+    int bm_words = 0;    // bitmap words per lane group
     // agent grid
     int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
         *cell_items = nullptr;
@@ -262,5 +270,6 @@ int device_debug_agents(Context& c, gmapf_v2* pos, int* state, int* cur, int* ta
 int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::string& err);
 int device_autotune(Context& c, std::string& err);
 int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
+int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, std::string& err);
 
 }  // namespace gmapf_b200

@@ -107,6 +107,28 @@ __global__ void k_apply_targets(const int4* recs, int n, int* state, int* targ_n
     targ_pos[r.x] = make_float2(__int_as_float(r.z), __int_as_float(r.w));
 }
 
+// device-resident retargets: locate each target on the device (the host
+// path's CuNodesMap::TryGetNodeIdx rule) and mark the agent Search
+__global__ void k_apply_targets_device(const int* ids, const float2* pos, int n, int A, LocateGrid loc,
+                                       int* state, int* targ_node, float2* targ_pos, int* err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int id = ids[k];
+    const float2 p = pos[k];
+    if (id < 0 || id >= A) {
+        atomicOr(err, ERR_BAD_REQUEST);
+        return;
+    }
+    const int node = locate(loc, p.x, p.y);
+    if (node < 0) {
+        atomicOr(err, ERR_BAD_REQUEST);
+        return;
+    }
+    state[id] = GMAPF_AGENT_SEARCH;
+    targ_node[id] = node;
+    targ_pos[id] = p;
+}
+
 __global__ void k_prepare_batch(const int* starts, const int* targets, int n, int nodes, int4* req,
                                 int* req_count, int* work_ctr, int* err) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -340,6 +362,14 @@ void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, i
                           float2* targ_pos) {
     if (n <= 0) return;
     k_apply_targets<<<blocks_for(n, 256), 256, 0, s>>>(recs, n, state, targ_node, targ_pos);
+}
+
+void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int A,
+                                 const LocateGrid& loc, int* state, int* targ_node, float2* targ_pos,
+                                 int* err) {
+    if (n <= 0) return;
+    k_apply_targets_device<<<blocks_for(n, 256), 256, 0, s>>>(ids, pos, n, A, loc, state, targ_node, targ_pos,
+                                                              err);
 }
 
 void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets, int n, int nodes,

@@ -2,8 +2,8 @@
 //
 // Method (reference: include/gmapf/PathFinder.h:138-251, CuQueue.h:33-70,
 // CuVisitedMap.h:45-54, path layout PathFinder.h:253-307):
-//   - one lane group of T threads (T in {2,4,8,16,32}, inside one warp) per
-//     path request; lane q owns bounded priority queue q of capacity C;
+//   - T lanes per path request (T in {2,4,8,16,32}); lane q owns bounded
+//     priority queue q of capacity C;
 //   - lane 0 is seeded with the start, lane 1 with the target (F = K*h(s,t));
 //   - each round every lane with a non-empty queue pops its minimum and
 //     expands up to three neighbours: G' = G+1, F' = G' + K*h where h is the
@@ -19,15 +19,26 @@
 // order is (F, G, node id); within a round candidates are taken slot-major
 // (neighbour slot 0 of lanes 0..T-1, then slot 1, then slot 2); the first
 // candidate of a node claims it and the first conflicting candidate is the
-// meeting pair.  Same-slot duplicates are resolved with __match_any_sync,
-// earlier-slot duplicates with the round's winner list in shared memory.
+// meeting pair.
 //
-// B200 layout: the per-lane queues are binary min-heaps in shared memory,
-// element k of thread t at [k * blockDim + t] (bank = lane: conflict-free);
-// the map is read as 48-byte SearchRows through the read-only path; visited
-// state is a 32-byte record per (slot, node) stamped with the query epoch so
-// nothing is cleared between queries; records carry six ancestors so the
-// path walk reads one record per six hops.
+// B200 mapping -- one warp per request:
+//   - threads 0..T-1 own the T queues (sorted rings in shared memory,
+//     maximum at the head and minimum at the tail: pop and eviction are O(1),
+//     an insertion moves only the entries smaller than the new one -- the
+//     reference's sorted array without its O(C) eviction shift);
+//   - candidate c = slot*T + lane of a round is handled by warp thread
+//     c mod 32 in pass c / 32 (one pass for T <= 8, two for T = 16, three for
+//     T = 32), so thread order is candidate order and a single
+//     __match_any_sync per pass resolves every claim of the pass: the lowest
+//     fresh thread of a node claims it, later ones see the claim;
+//   - visited state: a 2-bit-per-node bitmap (claimed, side) in shared memory
+//     when it fits, else a 32-byte record per (slot, node) in global memory
+//     stamped with the query epoch (no clearing between queries);
+//   - records (G, parent and five further ancestors) are written once per
+//     claimed node; the path walk reads one record per six hops;
+//   - rows of newly queued nodes are prefetched into L1, so the next round's
+//     expansion usually hits L1; idle warps refill from a device work counter
+//     (persistent form) or stop (plain form).
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -36,99 +47,85 @@ namespace gmapf_b200 {
 
 namespace {
 
-struct HeapRef {
-    float* F;
-    int* GD;
-    int* ID;
-    int stride;  // blockDim.x
-    int t;       // thread index
-    __device__ __forceinline__ int at(int k) const { return k * stride + t; }
-};
-
 // (F, G, id) lexicographic; gd = G << 1 | dir
 __device__ __forceinline__ bool key_less(float fa, int ga, int ia, float fb, int gb, int ib) {
     if (fa != fb) return fa < fb;
-    int Ga = ga >> 1, Gb = gb >> 1;
+    const int Ga = ga >> 1, Gb = gb >> 1;
     if (Ga != Gb) return Ga < Gb;
     return ia < ib;
 }
 
-__device__ __forceinline__ void heap_pop(const HeapRef& h, int& size, float& F, int& gd, int& id) {
-    F = h.F[h.at(0)];
-    gd = h.GD[h.at(0)];
-    id = h.ID[h.at(0)];
-    int n = --size;
-    if (n == 0) return;
-    float xf = h.F[h.at(n)];
-    int xg = h.GD[h.at(n)], xi = h.ID[h.at(n)];
-    int i = 0;
-    for (;;) {
-        int c = 2 * i + 1;
-        if (c >= n) break;
-        float cf = h.F[h.at(c)];
-        int cg = h.GD[h.at(c)], ci = h.ID[h.at(c)];
-        if (c + 1 < n) {
-            float df = h.F[h.at(c + 1)];
-            int dg = h.GD[h.at(c + 1)], di = h.ID[h.at(c + 1)];
-            if (key_less(df, dg, di, cf, cg, ci)) {
-                c = c + 1;
-                cf = df;
-                cg = dg;
-                ci = di;
-            }
-        }
-        if (!key_less(cf, cg, ci, xf, xg, xi)) break;
-        h.F[h.at(i)] = cf;
-        h.GD[h.at(i)] = cg;
-        h.ID[h.at(i)] = ci;
-        i = c;
+// A queued node: its key (F, G<<1|dir, id) and its five nearest ancestors,
+// which become ancestors 1..5 of the nodes it claims (so expanding it reads
+// no record from global memory).
+constexpr int kEntryWords = 8;
+
+// Per-lane sorted ring in shared memory: word w of entry k of lane q at
+// [(w*C + k)*T + q].
+struct Ring {
+    int* base;
+    int T;
+    int q;
+    int C;
+    __device__ __forceinline__ int at(int k) const {  // k in [0, 2C)
+        return (k >= C ? k - C : k) * T + q;
     }
-    h.F[h.at(i)] = xf;
-    h.GD[h.at(i)] = xg;
-    h.ID[h.at(i)] = xi;
+    __device__ __forceinline__ int* word(int w) const { return base + w * C * T; }
+};
+
+struct Entry {
+    float F;
+    int gd, id;
+    int a[5];
+};
+
+__device__ __forceinline__ void entry_load(const Ring& r, int k, Entry& e) {
+    e.F = __int_as_float(r.word(0)[k]);
+    e.gd = r.word(1)[k];
+    e.id = r.word(2)[k];
+#pragma unroll
+    for (int j = 0; j < 5; j++) e.a[j] = r.word(3 + j)[k];
 }
 
-__device__ __forceinline__ void heap_sift_up(const HeapRef& h, int i, float xf, int xg, int xi) {
-    while (i > 0) {
-        int p = (i - 1) >> 1;
-        float pf = h.F[h.at(p)];
-        int pg = h.GD[h.at(p)], pi = h.ID[h.at(p)];
-        if (!key_less(xf, xg, xi, pf, pg, pi)) break;
-        h.F[h.at(i)] = pf;
-        h.GD[h.at(i)] = pg;
-        h.ID[h.at(i)] = pi;
-        i = p;
-    }
-    h.F[h.at(i)] = xf;
-    h.GD[h.at(i)] = xg;
-    h.ID[h.at(i)] = xi;
+__device__ __forceinline__ void entry_store(const Ring& r, int k, const Entry& e) {
+    r.word(0)[k] = __float_as_int(e.F);
+    r.word(1)[k] = e.gd;
+    r.word(2)[k] = e.id;
+#pragma unroll
+    for (int j = 0; j < 5; j++) r.word(3 + j)[k] = e.a[j];
 }
 
-// Bounded push (CuQueue.h:33-63 with the (F,G,id) order): below capacity the
-// item is inserted; at capacity the maximum (always a leaf of the min-heap)
-// is replaced by the item when the item is smaller, else the item is dropped.
-__device__ __forceinline__ void heap_push(const HeapRef& h, int& size, int cap, float F, int gd,
-                                          int id) {
-    if (size < cap) {
-        heap_sift_up(h, size, F, gd, id);
-        size++;
-        return;
+// pop the minimum (element size-1; elements are kept in descending order);
+// returns the ring slot, whose ancestor words stay intact until this
+// round's pushes
+__device__ __forceinline__ int ring_pop(const Ring& r, int beg, int& size, int& gd, int& id) {
+    const int k = r.at(beg + size - 1);
+    gd = r.word(1)[k];
+    id = r.word(2)[k];
+    size--;
+    return k;
+}
+
+// bounded push (CuQueue.h:33-63 with the (F,G,id) order)
+__device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, const Entry& x) {
+    if (size == r.C) {
+        const int k0 = r.at(beg);
+        if (!key_less(x.F, x.gd, x.id, __int_as_float(r.word(0)[k0]), r.word(1)[k0], r.word(2)[k0]))
+            return;                            // not below the maximum: dropped
+        beg = (beg + 1 == r.C) ? 0 : beg + 1;  // evict the maximum
+        size--;
     }
-    int m = size >> 1;
-    float mf = h.F[h.at(m)];
-    int mg = h.GD[h.at(m)], mi = h.ID[h.at(m)];
-    for (int k = m + 1; k < size; k++) {
-        float kf = h.F[h.at(k)];
-        int kg = h.GD[h.at(k)], ki = h.ID[h.at(k)];
-        if (key_less(mf, mg, mi, kf, kg, ki)) {
-            m = k;
-            mf = kf;
-            mg = kg;
-            mi = ki;
-        }
+    int i = size - 1;
+    while (i >= 0) {
+        const int k = r.at(beg + i);
+        if (!key_less(__int_as_float(r.word(0)[k]), r.word(1)[k], r.word(2)[k], x.F, x.gd, x.id)) break;
+        Entry e;
+        entry_load(r, k, e);
+        entry_store(r, r.at(beg + i + 1), e);
+        i--;
     }
-    if (!key_less(F, gd, id, mf, mg, mi)) return;
-    heap_sift_up(h, m, F, gd, id);
+    entry_store(r, r.at(beg + i + 1), x);
+    size++;
 }
 
 __device__ __forceinline__ int2 ld_state(const Rec* r) {
@@ -146,43 +143,69 @@ __device__ __forceinline__ void st_rec(Rec* r, unsigned stamp, int gd, int a0, i
     __stcg(reinterpret_cast<int4*>(r) + 1, make_int4(a2, a3, a4, a5));
 }
 
-template <int T>
-__global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, int req_base) {
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// 2-bit visited state: bit 0 = claimed, bit 1 = reached from the start
+__device__ __forceinline__ int bm_get(const unsigned* bm, int n) {
+    return (int)((bm[n >> 4] >> ((n & 15) << 1)) & 3u);
+}
+__device__ __forceinline__ void bm_set(unsigned* bm, int n, int dir) {
+    atomicOr(bm + (n >> 4), (1u | ((unsigned)dir << 1)) << ((n & 15) << 1));
+}
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// per-warp shared-memory regions in 4-byte words, rounded to 16 bytes
+__host__ __device__ __forceinline__ size_t search_queue_words(int C, int T) {
+    return ((size_t)kEntryWords * C * T + 3) & ~(size_t)3;
+}
+__host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
+    return ((size_t)kEntryWords * 3 * T + 3) & ~(size_t)3;
+}
+
+__device__ __forceinline__ void prefetch_row(const SearchRow* rows, int id) {
+    const char* rp = reinterpret_cast<const char*>(rows + id);
+    prefetch_l1(rp);
+    prefetch_l1(rp + sizeof(SearchRow) - 1);
+}
+
+template <int T, bool SMEMV>
+__global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
+    constexpr int NP = (3 * T + 31) / 32;  // candidate passes per round
     extern __shared__ __align__(16) unsigned char smem[];
-    const int B = blockDim.x;
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int q = tid & (T - 1);
-    const int gbase_lane = lane & ~(T - 1);
-    const unsigned gmask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << gbase_lane);
-    const int C = p.C;
-    const int groups_per_block = B / T;
-    const int group = tid / T;
-    const int slot = blockIdx.x * groups_per_block + group;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;                 // warp in block
+    const int wpb = blockDim.x >> 5;                  // warps per block
+    const int slot = blockIdx.x * wpb + wib;          // one request slot per warp
     const int n_nodes = p.n;
-
-    HeapRef h;
-    h.F = reinterpret_cast<float*>(smem);
-    h.GD = reinterpret_cast<int*>(h.F + (size_t)C * B);
-    h.ID = h.GD + (size_t)C * B;
-    h.stride = B;
-    h.t = tid;
-    int* wId = h.ID + (size_t)C * B;
-    int* wGD = wId + 3 * B;
-    float* wF = reinterpret_cast<float*>(wGD + 3 * B);
-    const int wb = group * 3 * T;  // this group's winner list
-
-    if (slot >= p.slots) return;  // whole groups: slot is group-uniform
-    Rec* rec = p.rec + (size_t)slot * n_nodes;
     const float K = p.K;
+    const int C = p.C;
+
+    // shared memory: [queues of every warp][frontiers of every warp][bitmaps],
+    // each per-warp region a whole number of 16-byte words
+    const size_t qblk = search_queue_words(C, T), fblk = search_frontier_words(T);
+    int* base = reinterpret_cast<int*>(smem);
+    Ring ring;
+    ring.base = base + (size_t)wib * qblk;
+    ring.T = T;
+    ring.q = lane < T ? lane : 0;
+    ring.C = C;
+    int* fr = base + (size_t)wpb * qblk + (size_t)wib * fblk;  // word w of item i at fr[w*3T + i]
+    unsigned* bm = reinterpret_cast<unsigned*>(base + (size_t)wpb * (qblk + fblk)) + (size_t)wib * bm_words;
+
+    if (slot >= p.slots) return;  // whole warps
+    Rec* rec = p.rec + (size_t)slot * n_nodes;
+    const unsigned lt_mask = (1u << lane) - 1u;
 
     for (int iter = 0;; iter++) {
-        int r;
-        int R;
+        // ------------------------------------------------------------ fetch
+        int r, R;
         if (persistent) {
             int v = 0;
-            if (q == 0) v = atomicAdd(p.work_ctr, 1);
-            r = __shfl_sync(gmask, v, gbase_lane);
+            if (lane == 0) v = atomicAdd(p.work_ctr, 1);
+            r = __shfl_sync(kFull, v, 0);
             R = *p.req_count_d;
         } else {
             if (iter > 0) break;
@@ -190,244 +213,258 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
             R = p.req_count_h;
         }
         if (r >= R) break;
-
         const int4 rq = p.req[r];
         const int agent = rq.x, start = rq.y, target = rq.z, orow = rq.w;
-        if (start < 0 || start >= n_nodes || target < 0 || target >= n_nodes) {
-            if (q == 0) {
-                atomicOr(p.err, ERR_BAD_REQUEST);
-                if (p.out_found) p.out_found[r] = 0;
+        if (start < 0 || start >= n_nodes || target < 0 || target >= n_nodes || start == target) {
+            const bool bad = start != target || start < 0 || start >= n_nodes;
+            if (lane == 0) {  // bad request: not found; start == target: found, empty path
+                if (bad) atomicOr(p.err, ERR_BAD_REQUEST);
+                if (p.out_found) p.out_found[r] = bad ? 0 : 1;
                 if (p.out_len) p.out_len[r] = 0;
                 if (agent >= 0 && p.ag_state) {
                     p.ag_state[agent] = GMAPF_AGENT_IDLE;
                     p.ag_path_len[agent] = 0;
                 }
+                if (!bad) atomicAdd(p.stats + ST_FOUND, 1ull);
             }
             continue;
         }
 
-        if (start == target) {  // already there: found, empty path (never a step request)
-            if (q == 0) {
-                if (p.out_found) p.out_found[r] = 1;
-                if (p.out_len) p.out_len[r] = 0;
-                atomicAdd(p.stats + ST_FOUND, 1ull);
-            }
-            continue;
-        }
-
-        // epoch of this query in this slot (slot-private; no atomics needed)
         unsigned ep = 0;
-        if (q == 0) ep = p.epoch[slot] + 1u;
-        ep = __shfl_sync(gmask, ep, gbase_lane);
-        if (ep == 0u) {  // 2^32 queries in this slot: wipe its records once
-            for (long long k = q; k < (long long)n_nodes * 2; k += T)
-                __stcg(reinterpret_cast<int4*>(rec) + k, make_int4(0, 0, 0, 0));
-            __syncwarp(gmask);
-            ep = 1u;
+        if (!SMEMV) {
+            unsigned e = 0;
+            if (lane == 0) e = p.epoch[slot] + 1u;
+            e = __shfl_sync(kFull, e, 0);
+            if (e == 0u) {  // 2^32 queries in this slot: wipe its records once
+                for (long long k = lane; k < (long long)n_nodes * 2; k += 32)
+                    __stcg(reinterpret_cast<int4*>(rec) + k, make_int4(0, 0, 0, 0));
+                e = 1u;
+            }
+            if (lane == 0) p.epoch[slot] = e;
+            ep = e;
+        } else {
+            uint4* b4 = reinterpret_cast<uint4*>(bm);
+            for (int k = lane; k < (bm_words >> 2); k += 32) b4[k] = make_uint4(0, 0, 0, 0);
         }
-        if (q == 0) p.epoch[slot] = ep;
-
+        __syncwarp();
         const float2 cs = p.cen[start];
         const float2 ct = p.cen[target];
         const float f0 = GM_FMUL(dist_sqr(cs.x, cs.y, ct.x, ct.y), K);
-
-        int hsize = 0;
-        if (q == 0) {  // PathFinder.h:168-178
-            heap_push(h, hsize, C, f0, (0 << 1) | 1, start);
-            st_rec(rec + start, ep, 1, -1, -1, -1, -1, -1, -1);
-        } else if (q == 1) {  // PathFinder.h:179-189
-            heap_push(h, hsize, C, f0, (0 << 1) | 0, target);
-            st_rec(rec + target, ep, 0, -1, -1, -1, -1, -1, -1);
+        int qbeg = 0, qsize = 0;  // lanes < T: this lane's queue
+        if (lane < 2) {           // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
+            const int node = lane == 0 ? start : target;
+            Entry e;
+            e.F = f0;
+            e.gd = lane == 0 ? 1 : 0;
+            e.id = node;
+#pragma unroll
+            for (int j = 0; j < 5; j++) e.a[j] = -1;
+            ring_push(ring, qbeg, qsize, e);
+            st_rec(rec + node, ep, e.gd, -1, -1, -1, -1, -1, -1);
+            if (SMEMV) bm_set(bm, node, e.gd);
+            prefetch_row(p.rows, node);
         }
-        __syncwarp(gmask);
+        __syncwarp();
 
-        unsigned expansions = 0, deg_sum = 0, claims = (q == 0) ? 2u : 0u;
-        unsigned rounds = 0;
+        unsigned expansions = 0, deg_sum = 0, claims = 2, rounds = 0;
         int found = 0, mS = -1, gS = 0, mT = -1, gT = 0;
 
+        // ------------------------------------------------------------ rounds
         for (;;) {
             rounds++;
-            if ((int)rounds > p.max_rounds) {
-                if (q == 0) atomicOr(p.err, ERR_ROUNDS);
-                break;
-            }
-            const bool has = hsize > 0;
-            float Fu = 0.f;
-            int gdu = 0, idu = 0;
-            if (has) heap_pop(h, hsize, Fu, gdu, idu);
-
-            int deg = 0;
-            int nid0 = -1, nid1 = -1, nid2 = -1;
-            float nx0 = 0, ny0 = 0, nx1 = 0, ny1 = 0, nx2 = 0, ny2 = 0;
-            int4 ra = make_int4(0, 0, -1, -1), rb = make_int4(-1, -1, -1, -1);
-            if (has) {
-                const int4* rp = reinterpret_cast<const int4*>(p.rows + idu);
-                const int4 r0 = __ldg(rp);
-                const float4 r1 = __ldg(reinterpret_cast<const float4*>(rp + 1));
-                const float4 r2 = __ldg(reinterpret_cast<const float4*>(rp + 2));
-                ld_rec(rec + idu, ra, rb);
-                nid0 = r0.x;
-                nid1 = r0.y;
-                nid2 = r0.z;
-                deg = r0.w;
-                nx0 = r1.x;
-                ny0 = r1.y;
-                nx1 = r1.z;
-                ny1 = r1.w;
-                nx2 = r2.x;
-                ny2 = r2.y;
-                expansions++;
-                deg_sum += (unsigned)deg;
-            }
-            const int du = gdu & 1;
-            const int Gn = (gdu >> 1) + 1;
-            const int ngd = (Gn << 1) | du;
-            const float farx = du ? ct.x : cs.x;
-            const float fary = du ? ct.y : cs.y;
-
-            // previous-round claim state of every candidate (one L2 round trip)
-            int2 s0 = make_int2(0, 0), s1 = make_int2(0, 0), s2 = make_int2(0, 0);
-            if (deg > 0) s0 = ld_state(rec + nid0);
-            if (deg > 1) s1 = ld_state(rec + nid1);
-            if (deg > 2) s2 = ld_state(rec + nid2);
-            __syncwarp(gmask);  // every load of the round precedes every write
+            // lanes < T pop their minimum
+            int idu = -1, gdu = 0, uslot = 0;
+            if (lane < T && qsize > 0) uslot = ring_pop(ring, qbeg, qsize, gdu, idu);
 
             int nwin = 0;
             bool meet = false;
+            int mu = 0, mgu = 0, mn = 0, mgn = 0, mgn_known = 0;
 #pragma unroll
-            for (int s = 0; s < 3; s++) {
-                const int n = (s == 0) ? nid0 : (s == 1) ? nid1 : nid2;
-                const int2 st = (s == 0) ? s0 : (s == 1) ? s1 : s2;
-                const float cx = (s == 0) ? nx0 : (s == 1) ? nx1 : nx2;
-                const float cy = (s == 0) ? ny0 : (s == 1) ? ny1 : ny2;
-                const bool valid = s < deg;
-                bool prev = valid && (unsigned)st.x == ep;
-                int pgd = st.y;
-                if (valid && !prev) {  // claimed earlier in this round (earlier slot)
-                    for (int w = 0; w < nwin; w++) {
-                        if (wId[wb + w] == n) {
-                            prev = true;
-                            pgd = wGD[wb + w];
-                            break;
-                        }
+            for (int pass = 0; pass < NP; pass++) {
+                const int c = pass * 32 + lane;          // candidate order = slot * T + lane
+                const int s = c / T, qq = c - s * T;
+                const int cu = __shfl_sync(kFull, idu, qq & 31);
+                const int cgdu = __shfl_sync(kFull, gdu, qq & 31);
+                const int cslot = __shfl_sync(kFull, uslot, qq & 31);
+                bool valid = c < 3 * T && cu >= 0;
+                int n = -1;
+                float nx = 0.f, ny = 0.f;
+                if (valid) {
+                    const SearchRow* rw = p.rows + cu;
+                    const int4 r0 = __ldg(reinterpret_cast<const int4*>(rw));
+                    const float2 cc = __ldg(reinterpret_cast<const float2*>(&rw->x0) + s);
+                    n = (s == 0) ? r0.x : (s == 1) ? r0.y : r0.z;
+                    valid = s < r0.w;
+                    nx = cc.x;
+                    ny = cc.y;
+                    if (s == 0) {
+                        expansions++;
+                        deg_sum += (unsigned)r0.w;
+                    }
+                }
+                const int du = cgdu & 1;
+                const int ngd = (((cgdu >> 1) + 1) << 1) | du;
+                bool prev = false;
+                int pgd = 0, pknown = 0;
+                if (valid) {
+                    if (SMEMV) {
+                        const int st = bm_get(bm, n);  // includes earlier passes of this round
+                        prev = (st & 1) != 0;
+                        pgd = st >> 1;                 // side only; G read at the meet
+                    } else {
+                        // sees claims of earlier passes too: their record stores are
+                        // ordered before this load by the pass's __syncwarp
+                        const int2 st = ld_state(rec + n);
+                        prev = (unsigned)st.x == ep;
+                        pgd = st.y;
+                        pknown = 1;
                     }
                 }
                 const bool fresh = valid && !prev;
-                const int key = fresh ? n : (-1 - lane);
-                const unsigned mm = __match_any_sync(gmask, key);
+                const unsigned mm = __match_any_sync(kFull, fresh ? n : (-1 - lane));
                 const int leader = __ffs(mm) - 1;
                 const bool win = fresh && leader == lane;
-                const int lgd = __shfl_sync(gmask, ngd, leader);
-                int cgd = 0;
+                const int lgd = __shfl_sync(kFull, ngd, leader);
                 bool conflict = false;
+                int cgd = 0, cknown = 1;
                 if (fresh && !win) {
                     cgd = lgd;
                     conflict = (lgd & 1) != du;
                 } else if (prev) {
                     cgd = pgd;
-                    conflict = (pgd & 1) != du;
+                    cknown = pknown;
+                    conflict = (SMEMV ? pgd : (pgd & 1)) != du;
                 }
-                const unsigned cm = __ballot_sync(gmask, conflict) & gmask;
-                if (!meet && cm != 0u) {  // group-uniform
+                const unsigned cm = __ballot_sync(kFull, conflict);
+                if (!meet && cm != 0u) {  // warp-uniform
                     const int ml = __ffs(cm) - 1;
-                    const int mu = __shfl_sync(gmask, idu, ml);
-                    const int mgu = __shfl_sync(gmask, gdu, ml);
-                    const int mn = __shfl_sync(gmask, n, ml);
-                    const int mgn = __shfl_sync(gmask, cgd, ml);
-                    if (mgu & 1) {  // PathFinder.h:226-227
-                        mS = mu;
-                        gS = mgu >> 1;
-                        mT = mn;
-                        gT = mgn >> 1;
-                    } else {
-                        mS = mn;
-                        gS = mgn >> 1;
-                        mT = mu;
-                        gT = mgu >> 1;
-                    }
+                    mu = __shfl_sync(kFull, cu, ml);
+                    mgu = __shfl_sync(kFull, cgdu, ml);
+                    mn = __shfl_sync(kFull, n, ml);
+                    mgn = __shfl_sync(kFull, cgd, ml);
+                    mgn_known = __shfl_sync(kFull, cknown, ml);
                     meet = true;
                 }
-                const unsigned wm = __ballot_sync(gmask, win) & gmask;
+                const unsigned wm = __ballot_sync(kFull, win);
                 if (win) {
-                    const int idx = nwin + __popc(wm & ((1u << lane) - 1u));
-                    const float hh = dist_sqr(cx, cy, farx, fary);
-                    const float F = GM_FADD((float)Gn, GM_FMUL(hh, K));
-                    wId[wb + idx] = n;
-                    wGD[wb + idx] = ngd;
-                    wF[wb + idx] = F;
-                    st_rec(rec + n, ep, ngd, idu, ra.z, ra.w, rb.x, rb.y, rb.z);
+                    const int idx = nwin + __popc(wm & lt_mask);
+                    const float farx = du ? ct.x : cs.x;
+                    const float fary = du ? ct.y : cs.y;
+                    const float hh = dist_sqr(nx, ny, farx, fary);
+                    const float F = GM_FADD((float)(ngd >> 1), GM_FMUL(hh, K));
+                    // ancestors 1..5 of n = the popped node's ancestors 0..4 (its queue slot)
+                    int ua[5];
+#pragma unroll
+                    for (int j = 0; j < 5; j++) ua[j] = ring.base[(3 + j) * C * T + cslot];
+                    fr[0 * 3 * T + idx] = __float_as_int(F);
+                    fr[1 * 3 * T + idx] = ngd;
+                    fr[2 * 3 * T + idx] = n;
+                    fr[3 * 3 * T + idx] = cu;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) fr[(4 + j) * 3 * T + idx] = ua[j];
+                    if (SMEMV) bm_set(bm, n, du);
+                    st_rec(rec + n, ep, ngd, cu, ua[0], ua[1], ua[2], ua[3], ua[4]);
+                    // the rows this node's expansion will read next: its neighbours'
+                    const int* gg = p.rows[cu].g + 3 * s;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        const int m = __ldg(gg + j);
+                        if (m >= 0 && m != cu) prefetch_row(p.rows, m);
+                    }
                 }
                 nwin += __popc(wm);
-                __syncwarp(gmask);
+                __syncwarp();
             }
-            if (q == 0) claims += (unsigned)nwin;
+            claims += (unsigned)nwin;
+            bool ended = false;
             if (meet) {
+                if (!mgn_known) {  // side came from the bitmap: read G from the record
+                    int g = 0;
+                    if (lane == 0) g = ld_state(rec + mn).y;
+                    mgn = __shfl_sync(kFull, g, 0);
+                }
+                if (mgu & 1) {  // PathFinder.h:226-227
+                    mS = mu;
+                    gS = mgu >> 1;
+                    mT = mn;
+                    gT = mgn >> 1;
+                } else {
+                    mS = mn;
+                    gS = mgn >> 1;
+                    mT = mu;
+                    gT = mgu >> 1;
+                }
                 found = 1;
-                break;
+                ended = true;
+            } else {
+                if (lane < T) {
+                    for (int i = lane; i < nwin; i += T) {
+                        Entry e;
+                        e.F = __int_as_float(fr[i]);
+                        e.gd = fr[3 * T + i];
+                        e.id = fr[2 * 3 * T + i];
+#pragma unroll
+                        for (int j = 0; j < 5; j++) e.a[j] = fr[(3 + j) * 3 * T + i];
+                        ring_push(ring, qbeg, qsize, e);
+                    }
+                }
+                if (!__any_sync(kFull, qsize > 0)) ended = true;
+                if ((int)rounds >= p.max_rounds) {
+                    if (lane == 0) atomicOr(p.err, ERR_ROUNDS);
+                    ended = true;
+                }
             }
-            for (int i = q; i < nwin; i += T) heap_push(h, hsize, C, wF[wb + i], wGD[wb + i], wId[wb + i]);
-            const bool any = __any_sync(gmask, hsize > 0);
-            __syncwarp(gmask);  // winner list reads done before the next round
-            if (!any) break;
+            __syncwarp();  // frontier reads done before the next round rewrites it
+            if (ended) break;
         }
 
-        // path reconstruction (PathFinder.h:276-306)
+        // ------------------------------------------------------------ path walk
         int L = 0;
         if (found) {
             L = gS + gT + 1;
             const int row = (agent >= 0) ? agent : orow;
             if ((long long)L > p.path_stride) {
-                if (q == 0) atomicOr(p.err, ERR_PATH_CAP);
-            } else {
+                if (lane == 0) atomicOr(p.err, ERR_PATH_CAP);
+            } else if (lane < 2) {
                 int* out = p.paths + (long long)row * p.path_stride;
-                if (q == 0) {
-                    // start side: depths gS..1 at positions gS-1..0
-                    int x = mS, g = gS;
+                // lane 0: start side, depths gS..1 at positions gS-1..0
+                // lane 1: target side, depths gT..0 at positions gS..gS+gT
+                int x = lane == 0 ? mS : mT;
+                int g = lane == 0 ? gS : gT;
+                const int stop = lane == 0 ? 1 : 0;
+                if (lane == 0) {
                     if (g >= 1) out[g - 1] = x;
-                    while (g > 1) {
-                        if (x < 0 || x >= n_nodes) {
-                            atomicOr(p.err, ERR_BOUNDS);
-                            break;
-                        }
-                        int4 a, b;
-                        ld_rec(rec + x, a, b);
-                        const int anc[6] = {a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-                        for (int j = 0; j < 6; j++) {
-                            const int d = g - 1 - j;
-                            if (d >= 1) out[d - 1] = anc[j];
-                        }
-                        x = anc[5];
-                        g -= 6;
-                    }
-                } else if (q == 1) {
-                    // target side: depths gT..0 at positions gS..gS+gT
-                    int x = mT, g = gT;
+                } else {
                     out[gS] = x;
-                    while (g > 0) {
-                        if (x < 0 || x >= n_nodes) {
-                            atomicOr(p.err, ERR_BOUNDS);
-                            break;
-                        }
-                        int4 a, b;
-                        ld_rec(rec + x, a, b);
-                        const int anc[6] = {a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-                        for (int j = 0; j < 6; j++) {
-                            const int d = g - 1 - j;
-                            if (d >= 0) out[gS + gT - d] = anc[j];
-                        }
-                        x = anc[5];
-                        g -= 6;
+                }
+                while (g > stop) {
+                    if (x < 0 || x >= n_nodes) {
+                        atomicOr(p.err, ERR_BOUNDS);
+                        break;
                     }
+                    int4 a, b;
+                    ld_rec(rec + x, a, b);
+                    const int anc[6] = {a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+                    for (int j = 0; j < 6; j++) {
+                        const int d = g - 1 - j;
+                        if (d >= stop) {
+                            if (lane == 0)
+                                out[d - 1] = anc[j];
+                            else
+                                out[gS + gT - d] = anc[j];
+                        }
+                    }
+                    x = anc[5];
+                    g -= 6;
                 }
             }
         }
-        __syncwarp(gmask);
+        __syncwarp();
         // results, agent update (PathFinder.h:268-289) and counters
-        const unsigned ex = __reduce_add_sync(gmask, expansions);
-        const unsigned ds = __reduce_add_sync(gmask, deg_sum);
-        if (q == 0) {
+        const unsigned ex = __reduce_add_sync(kFull, expansions);
+        const unsigned ds = __reduce_add_sync(kFull, deg_sum);
+        if (lane == 0) {
             if (p.out_found) p.out_found[r] = found;
             if (p.out_len) p.out_len[r] = L;
             if (agent >= 0 && p.ag_state) {
@@ -445,70 +482,81 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
     }
 }
 
-template <int T>
+template <int T, bool SMEMV>
 cudaError_t launch_t(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
-                     int req_base) {
-    // the dynamic shared-memory limit was raised by search_max_blocks_per_sm
-    // when the search state was sized (no attribute calls here: this may run
-    // under stream capture)
-    size_t smem = search_smem_bytes(T, p.C, bt);
+                     int req_base, int bm_words) {
+    // the dynamic shared-memory limit was raised when the search state was
+    // sized (no attribute calls here: this may run under stream capture)
+    const size_t smem = search_smem_bytes(p.C, bt, SMEMV ? bm_words : 0, T);
     if (blocks <= 0) return cudaSuccess;
-    k_search<T><<<blocks, bt, smem, s>>>(p, persistent ? 1 : 0, req_base);
+    k_search<T, SMEMV><<<blocks, bt, smem, s>>>(p, persistent ? 1 : 0, req_base, bm_words);
     return cudaGetLastError();
 }
 
-}  // namespace
-
-size_t search_smem_bytes(int T, int C, int bt) {
-    (void)T;
-    return (size_t)C * bt * 12 + (size_t)3 * bt * 12;
-}
-
-int search_max_blocks_per_sm(int T, int C, int bt) {
-    int nb = 0;
-    size_t smem = search_smem_bytes(T, C, bt);
-    cudaError_t e = cudaSuccess;
-    switch (T) {
-        case 2:
-            cudaFuncSetAttribute(k_search<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<2>, bt, smem);
-            break;
-        case 4:
-            cudaFuncSetAttribute(k_search<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<4>, bt, smem);
-            break;
-        case 8:
-            cudaFuncSetAttribute(k_search<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<8>, bt, smem);
-            break;
-        case 16:
-            cudaFuncSetAttribute(k_search<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<16>, bt, smem);
-            break;
-        case 32:
-            cudaFuncSetAttribute(k_search<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<32>, bt, smem);
-            break;
-        default:
-            return 0;
+template <int T, bool SMEMV>
+int occupancy_t(int C, int bt, int bm_words) {
+    const size_t smem = search_smem_bytes(C, bt, SMEMV ? bm_words : 0, T);
+    if (smem > 227 * 1024) return 0;
+    if (cudaFuncSetAttribute(k_search<T, SMEMV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
-    if (e != cudaSuccess) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<T, SMEMV>, bt, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     return nb;
 }
 
-cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
-                          int req_base) {
+template <bool SMEMV>
+cudaError_t launch_v(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
+                     int req_base, int bm_words) {
     switch (p.T) {
-        case 2: return launch_t<2>(s, p, blocks, bt, persistent, req_base);
-        case 4: return launch_t<4>(s, p, blocks, bt, persistent, req_base);
-        case 8: return launch_t<8>(s, p, blocks, bt, persistent, req_base);
-        case 16: return launch_t<16>(s, p, blocks, bt, persistent, req_base);
-        case 32: return launch_t<32>(s, p, blocks, bt, persistent, req_base);
+        case 2: return launch_t<2, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 4: return launch_t<4, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 8: return launch_t<8, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 16: return launch_t<16, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 32: return launch_t<32, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
         default: return cudaErrorInvalidValue;
     }
+}
+
+template <bool SMEMV>
+int occupancy_v(int T, int C, int bt, int bm_words) {
+    switch (T) {
+        case 2: return occupancy_t<2, SMEMV>(C, bt, bm_words);
+        case 4: return occupancy_t<4, SMEMV>(C, bt, bm_words);
+        case 8: return occupancy_t<8, SMEMV>(C, bt, bm_words);
+        case 16: return occupancy_t<16, SMEMV>(C, bt, bm_words);
+        case 32: return occupancy_t<32, SMEMV>(C, bt, bm_words);
+        default: return 0;
+    }
+}
+
+}  // namespace
+
+// per-block dynamic shared memory, per warp: T queues of C entries (12 B),
+// a frontier of 3T entries (12 B) and, on-chip mode, the visited bitmap
+size_t search_smem_bytes(int C, int bt, int bm_words_per_warp, int T) {
+    const size_t warps = (size_t)bt / 32;
+    return warps * 4 * (search_queue_words(C, T) + search_frontier_words(T) + (size_t)bm_words_per_warp);
+}
+
+int search_bitmap_words(int n_nodes) {
+    const int w = (n_nodes + 15) / 16;
+    return (w + 3) & ~3;  // whole uint4 for the clear
+}
+
+int search_max_blocks_per_sm(int T, int C, int bt, bool smem_visited, int bm_words) {
+    return smem_visited ? occupancy_v<true>(T, C, bt, bm_words) : occupancy_v<false>(T, C, bt, 0);
+}
+
+cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
+                          int req_base, bool smem_visited, int bm_words) {
+    return smem_visited ? launch_v<true>(s, p, blocks, bt, persistent, req_base, bm_words)
+                        : launch_v<false>(s, p, blocks, bt, persistent, req_base, 0);
 }
 
 }  // namespace gmapf_b200

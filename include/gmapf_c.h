@@ -87,7 +87,8 @@ typedef struct gmapf_options {
     int32_t autotune;          /* 1: pick threads/agent, queue capacity and block size per map at start */
     int64_t search_mem_budget; /* bytes for per-slot search records, 0 = automatic */
     int32_t order_by_estimate; /* 1: serve long searches first (results do not depend on it) */
-    int32_t _reserved[5];
+    int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records */
+    int32_t _reserved[4];
 } gmapf_options;
 
 typedef struct gmapf_step_stats {
@@ -134,6 +135,12 @@ gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id);
 gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t agent_id, float x, float y);
 /* bulk form of the above: n targets, one call */
 gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* pos, int32_t n);
+/* device-resident form: ids and positions already in device memory; the
+ * target triangles are located on the device (same rule as the host path).
+ * Enqueued on the context's stream before the next step; a position in no
+ * triangle leaves that agent unchanged and makes the next step report
+ * GMAPF_E_DEVICE.  Call after the start, not during a step. */
+gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_ids, const gmapf_v2* d_pos, int32_t n);
 
 /* GMAPF::ManualStart()                   -- src/GMAPF.cu:72-130 */
 gmapf_status gmapf_manual_start(gmapf_ctx* ctx);
@@ -175,6 +182,14 @@ gmapf_status gmapf_step_time_percentile(gmapf_ctx* ctx, float q, float* out_ms);
 gmapf_status gmapf_reset_profiler(gmapf_ctx* ctx);
 /* number of kernel launches issued by the library since creation */
 int64_t gmapf_kernel_launches(gmapf_ctx* ctx);
+/* the CUDA stream (cudaStream_t) the library launches on, for callers that
+ * time or order their own work against it; null before the start */
+void* gmapf_stream_handle(gmapf_ctx* ctx);
+/* effective search shape after the start: threads per agent, queue
+ * capacity, block size, visited mode (1 shared bitmap, 2 global records)
+ * and resident lane-group slots */
+gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t* block_threads,
+                                int32_t* visited_mode, int32_t* slots);
 
 /* ---- batched query API: searches only, no agents ---- */
 /* Run n independent searches (start/target node ids) with the context's

@@ -123,16 +123,18 @@ class OMap:
         return f, path[:L.value].copy(), st.as_dict()
 
     def search_batch(self, starts, targets, T, Cap, K=1.0, threads=None, path_stride=None):
+        """path_stride=0: lengths and counters only, no path rows."""
         s = np.ascontiguousarray(starts, np.int32)
         t = np.ascontiguousarray(targets, np.int32)
         n = len(s)
-        stride = path_stride or max(1, self.n)
+        stride = max(1, self.n) if path_stride is None else path_stride
         found = np.empty(n, np.int32)
         lens = np.empty(n, np.int32)
-        paths = np.full((n, stride), -1, np.int32)
+        paths = np.full((n, stride), -1, np.int32) if stride > 0 else None
         st = SearchStats()
         rc = self.lib.orc_search_batch(self.h, _p(s), _p(t), n, int(T), int(Cap), float(K), _p(found), _p(lens),
-                                       _p(paths), stride, C.byref(st), int(threads or os.cpu_count() or 1))
+                                       _p(paths) if paths is not None else None, stride, C.byref(st),
+                                       int(threads or os.cpu_count() or 1))
         if rc != 0:
             raise RuntimeError("oracle path row too small")
         return found, lens, paths, st.as_dict()

@@ -28,28 +28,31 @@ def check_batch(oracle_mod, g, starts, targets, T, Cap, K=1.0):
     return f, l, p, st
 
 
+@pytest.mark.parametrize("vm", [1, 2])
 @pytest.mark.parametrize("T,Cap", [(2, 1), (2, 16), (4, 16), (8, 2), (32, 64)])
-def test_cfg1_all_pairs(oracle_mod, T, Cap):
+def test_cfg1_all_pairs(oracle_mod, T, Cap, vm):
     scn = S.cfg1()
-    g = map_world(scn, T=T, Cap=Cap)
+    g = map_world(scn, T=T, Cap=Cap, visited_mode=vm)
     n = g.node_count
     s, t = np.meshgrid(np.arange(n), np.arange(n))
     f, l, p, st = check_batch(oracle_mod, g, s.ravel().astype(np.int32), t.ravel().astype(np.int32), T, Cap)
     assert f.mean() > 0.5
 
 
+@pytest.mark.parametrize("vm", [1, 2])
 @pytest.mark.parametrize("T,Cap", [(8, 32), (4, 16), (16, 8)])
-def test_cfg2_random(oracle_mod, T, Cap):
+def test_cfg2_random(oracle_mod, T, Cap, vm):
     scn = S.cfg2()
-    g = map_world(scn, T=T, Cap=Cap)
+    g = map_world(scn, T=T, Cap=Cap, visited_mode=vm)
     s, t = random_queries(g, scn, 2048, seed=11)
     check_batch(oracle_mod, g, s, t, T, Cap)
 
 
+@pytest.mark.parametrize("vm", [1, 2])
 @pytest.mark.parametrize("T,Cap", [(8, 32), (32, 64), (2, 256)])
-def test_maze64_random(oracle_mod, T, Cap):
+def test_maze64_random(oracle_mod, T, Cap, vm):
     scn = S.cfg3(cells=64)
-    g = map_world(scn, T=T, Cap=Cap)
+    g = map_world(scn, T=T, Cap=Cap, visited_mode=vm)
     s, t = random_queries(g, scn, 512, seed=12)
     f, l, p, st = check_batch(oracle_mod, g, s, t, T, Cap)
     # path validity: consecutive triangles are neighbours and the path ends at the target
@@ -62,10 +65,11 @@ def test_maze64_random(oracle_mod, T, Cap):
                 assert b in nb[a]
 
 
-def test_plain_equals_batched(oracle_mod):
+@pytest.mark.parametrize("vm", [1, 2])
+def test_plain_equals_batched(oracle_mod, vm):
     scn = S.cfg2()
-    gb = map_world(scn, T=8, Cap=32, mode=G.MODE_BATCHED)
-    gp = map_world(scn, T=8, Cap=32, mode=G.MODE_PLAIN)
+    gb = map_world(scn, T=8, Cap=32, mode=G.MODE_BATCHED, visited_mode=vm)
+    gp = map_world(scn, T=8, Cap=32, mode=G.MODE_PLAIN, visited_mode=3 - vm)
     s, t = random_queries(gb, scn, 1500, seed=13)
     fb, lb, pb, _ = gb.search_batch(s, t, gb.node_count)
     fp, lp, pp, _ = gp.search_batch(s, t, gp.node_count)

@@ -10,9 +10,9 @@ from gpu_util import close_rel
 pytestmark = pytest.mark.gpu
 
 
-def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None):
+def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None, vm=0):
     g, starts, rng = S.make_world(scn, mode=mode, agents=agents, threads_per_agent=T, queue_capacity=Cap,
-                                  parallel_agents=P)
+                                  parallel_agents=P, visited_mode=vm)
     om = oracle_mod.OMap(g.map_nodes())
     ow = oracle_mod.OWorld(om, agents, scn.radius, scn.speed, P or agents, T or scn.threads_per_agent,
                            Cap or scn.queue_capacity, scn.heuristic_k)
@@ -68,9 +68,10 @@ def test_cfg1_200_steps(oracle_mod):
     assert np.array_equal(pos, d["pos"], equal_nan=True)
 
 
-def test_cfg2_retargets(oracle_mod):
+@pytest.mark.parametrize("vm", [1, 2])
+def test_cfg2_retargets(oracle_mod, vm):
     scn = S.cfg2()
-    g, ow, rng = make_pair(oracle_mod, scn, 512)
+    g, ow, rng = make_pair(oracle_mod, scn, 512, vm=vm)
     run(g, ow, scn, 250, rng, retarget_every=100, check_every=25)
 
 
