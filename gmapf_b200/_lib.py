@@ -120,6 +120,9 @@ SIGNATURES = {
     "gmapf_search_batch_device": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(StepStats)]),
     "gmapf_last_search_ms": (C.c_int, [P, C.POINTER(C.c_float)]),
+    "gmapf_search_batch_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
+                                             C.c_int32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                             C.c_void_p]),
 }
 
 _lib = None

@@ -77,6 +77,10 @@ gmapf_status start_if_needed(Context& c) {
 
 }  // namespace
 
+namespace gmapf_b200 {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace gmapf_b200
+
 extern "C" {
 
 const char* gmapf_last_error(void) { return g_err.c_str(); }

@@ -272,4 +272,7 @@ int device_autotune(Context& c, std::string& err);
 int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
 int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, std::string& err);
 
+// capi.cpp: message returned by gmapf_last_error() on this thread
+void set_last_error(const std::string& msg);
+
 }  // namespace gmapf_b200

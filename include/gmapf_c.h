@@ -208,6 +208,30 @@ gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, 
  * events on the launching stream */
 gmapf_status gmapf_last_search_ms(gmapf_ctx* ctx, float* out_ms);
 
+/* ---- searches without any memory allocation ----
+ * No counterpart in the reference.  For callers that may not allocate
+ * device memory themselves or through the library (an engine that owns every
+ * GPU allocation, memory fully reserved, allocation not allowed at the point
+ * of the call): no context, no cudaMalloc, no cudaFree.  The caller passes
+ * the navmesh (n_nodes gmapf_node records, neighbours packed and -1 padded,
+ * as for FillMapManually; centroids are recomputed), the start/target
+ * triangle ids and the outputs, all in device memory; results equal
+ * gmapf_search_batch_device's for the same threads per agent and queue
+ * capacity.  found[i] is 1, 0, or -1 for an id outside the navmesh; a length
+ * above path_stride means path row i was left unwritten.
+ * Working memory is one 64 MiB array built into the library (held by every
+ * GPU that loads it until exit): the navmesh may have at most 2,097,144
+ * triangles, and fewer triangles give more concurrent requests.  Calls share
+ * that array: calls that overlap on the GPU race and must be serialized.
+ * Enqueued on `stream` (a cudaStream_t, null for the default stream) and
+ * asynchronous.  The first call on each device sets up the array's address
+ * and the kernel attributes, so make it before any stream capture.  Errors
+ * are read with gmapf_last_error(). */
+gmapf_status gmapf_search_batch_noalloc(const gmapf_node* d_nodes, int32_t n_nodes, const int32_t* d_starts,
+                                        const int32_t* d_targets, int32_t n_queries, int32_t threads_per_agent,
+                                        int32_t queue_capacity, float heuristic_k, int32_t* d_found,
+                                        int32_t* d_lens, int32_t* d_paths, int32_t path_stride, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
