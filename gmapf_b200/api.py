@@ -144,7 +144,7 @@ class GMAPF:
 
     # -- extras ------------------------------------------------------------
     def set_options(self, mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0,
-                    autotune: bool = False, search_mem_budget: int = 0, order_by_estimate: bool = False,
+                    autotune: bool = False, search_mem_budget: int = 0, order_by_estimate: bool = True,
                     visited_mode: int = 0) -> None:
         o = Options()
         o.device = device

@@ -91,6 +91,7 @@ gmapf_status gmapf_create(gmapf_ctx** out) {
     if (!*out) return fail(GMAPF_E_CAPACITY, "out of host memory");
     (*out)->c.opt.device = 0;
     (*out)->c.opt.mode = GMAPF_MODE_BATCHED;
+    (*out)->c.opt.order_by_estimate = 1;
     return GMAPF_OK;
 }
 

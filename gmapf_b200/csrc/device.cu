@@ -249,8 +249,12 @@ int enqueue_frame(Context& c, bool timing, std::string& err) {
     if (timing) CK(cudaEventRecordWithFlags(d.ev[1], s, cudaEventRecordExternal));
     CK(cudaEventRecord(d.ev[5], s));
     CK(cudaStreamWaitEvent(s2, d.ev[5], 0));
-    // search branch
+    // search branch (requests longest-first when the landmark estimate is on)
     SearchParams sp = search_params(c);
+    if (d.lm) {
+        launch_order_requests(s, d.req, d.counters + CT_REQ, d.req_sorted, d.req_keys, d.lm, d.lm_count, c.map.n);
+        sp.req = d.req_sorted;
+    }
     CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.smemv, d.bm_words));
     if (timing) CK(cudaEventRecordWithFlags(d.ev[2], s, cudaEventRecordExternal));
     // mover branch
@@ -295,7 +299,7 @@ int capture_graph(Context& c, std::string& err) {
     return GMAPF_OK;
 }
 
-int kernels_per_frame(Context& c) { return 2 + (c.A > 0 ? 4 : 0); }
+int kernels_per_frame(Context& c) { return 2 + (c.dev.lm ? 1 : 0) + (c.A > 0 ? 4 : 0); }
 
 }  // namespace
 
@@ -354,6 +358,16 @@ int device_start(Context& c, std::string& err) {
     DALLOC(d.paths, (size_t)std::max(1, A) * d.path_stride);
     DALLOC(d.req, std::max(1, c.cfg.PathFinderParallelAgents));
     DALLOC(d.counters, CT_COUNT);
+    if (c.opt.order_by_estimate && c.opt.mode == GMAPF_MODE_BATCHED && n > 0) {
+        // landmark hop distances for the longest-first request order
+        std::vector<unsigned short> lm;
+        d.lm_count = 8;
+        landmark_distances(m, d.lm_count, lm);
+        DALLOC(d.lm, lm.size());
+        CK(cudaMemcpy(d.lm, lm.data(), sizeof(unsigned short) * lm.size(), cudaMemcpyHostToDevice));
+        DALLOC(d.req_sorted, std::max(1, c.cfg.PathFinderParallelAgents));
+        DALLOC(d.req_keys, std::max(1, c.cfg.PathFinderParallelAgents));
+    }
     DALLOC(d.stats, ST_COUNT);
 
     std::vector<float2> tp(A);
@@ -584,12 +598,19 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
     cudaStream_t s = d.stream;
     CK(cudaSetDevice(d.device));
     if (n > d.breq_cap) {
-        if (d.breq) {
-            cudaFree(d.breq);
-            d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), (void*)d.breq), d.allocs.end());
+        for (void* p : {(void*)d.breq, (void*)d.breq_sorted, (void*)d.breq_keys}) {
+            if (!p) continue;
+            cudaFree(p);
+            d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), p), d.allocs.end());
         }
         d.breq = nullptr;
+        d.breq_sorted = nullptr;
+        d.breq_keys = nullptr;
         DALLOC(d.breq, (size_t)n);
+        if (d.lm) {
+            DALLOC(d.breq_sorted, (size_t)n);
+            DALLOC(d.breq_keys, (size_t)n);
+        }
         d.breq_cap = n;
     }
     CK(cudaMemsetAsync(d.counters + CT_ERR, 0, sizeof(int), s));
@@ -602,6 +623,11 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
     c.launches += 1;
     SearchParams sp = search_params(c);
     sp.req = d.breq;
+    if (d.lm && n > 0) {
+        launch_order_requests(s, d.breq, d.counters + CT_REQ, d.breq_sorted, d.breq_keys, d.lm, d.lm_count, c.map.n);
+        c.launches += 1;
+        sp.req = d.breq_sorted;
+    }
     sp.paths = d_paths;
     sp.path_stride = path_stride;
     sp.out_found = d_found;

@@ -33,18 +33,15 @@ namespace gmapf_b200 {
 constexpr int kInvalid = -1;
 
 // Per-node search row: the node's neighbours (packed, -1 padded) with the
-// count of leading valid ones, each neighbour's centroid, and each
-// neighbour's own neighbour ids (g[i][j] = neighbour j of neighbour i), so
-// that claiming a node can prefetch the rows its expansion will need.
-// 80 bytes, 16-byte aligned.
+// count of leading valid ones and each neighbour's centroid.  48 bytes,
+// 16-byte aligned: expanding a node reads one row.
 struct __align__(16) SearchRow {
     int n0, n1, n2, deg;
     float x0, y0, x1, y1;
     float x2, y2;
-    int g[9];
-    int pad;
+    int pad0, pad1;
 };
-static_assert(sizeof(SearchRow) == 80, "search row layout");
+static_assert(sizeof(SearchRow) == 48, "search row layout");
 
 // Point-location grid: every non-degenerate triangle is listed, in ascending
 // id, in each cell its padded bounding box touches; degenerate triangles

@@ -69,10 +69,7 @@ void build_host_map(const gmapf_node* nodes, int n, HostMap& m) {
         r.y1 = c1.y;
         r.x2 = c2.x;
         r.y2 = c2.y;
-        for (int k = 0; k < 3; k++)
-            for (int j = 0; j < 3; j++)
-                r.g[3 * k + j] = nb[k] >= 0 ? m.nodes[nb[k]].NeibsIdx[j] : -1;
-        r.pad = 0;
+        r.pad0 = r.pad1 = 0;
         m.rows[i] = r;
     }
 
@@ -139,6 +136,54 @@ void build_host_map(const gmapf_node* nodes, int n, HostMap& m) {
         range(i, a, b, c, d);
         for (int y = b; y <= d; y++)
             for (int x = a; x <= c; x++) m.glist[fill[(size_t)y * m.gw + x]++] = i;
+    }
+}
+
+}  // namespace gmapf_b200
+
+namespace gmapf_b200 {
+
+// Breadth-first hop distances over the search's neighbour lists (leading
+// valid entries).  Used only to order requests longest-first; the order
+// does not change any result.
+static void bfs_hops(const HostMap& m, int src, std::vector<unsigned short>& d) {
+    d.assign(m.n, 65535);
+    std::vector<int> q;
+    q.reserve(m.n);
+    d[src] = 0;
+    q.push_back(src);
+    for (size_t h = 0; h < q.size(); h++) {
+        const int u = q[h];
+        const SearchRow& r = m.rows[u];
+        const int nb[3] = {r.n0, r.n1, r.n2};
+        for (int k = 0; k < r.deg; k++) {
+            const int v = nb[k];
+            if (d[v] == 65535) {
+                d[v] = (unsigned short)std::min(65534, d[u] + 1);
+                q.push_back(v);
+            }
+        }
+    }
+}
+
+void landmark_distances(const HostMap& m, int count, std::vector<unsigned short>& out) {
+    out.assign((size_t)count * std::max(0, m.n), 65535);
+    if (m.n == 0 || count <= 0) return;
+    std::vector<unsigned short> d;
+    std::vector<unsigned> best(m.n, 0xffffffffu);  // distance to the nearest landmark so far
+    bfs_hops(m, 0, d);
+    int next = 0;
+    for (int i = 0; i < m.n; i++)
+        if (d[i] != 65535 && d[i] > d[next]) next = i;
+    for (int l = 0; l < count; l++) {
+        bfs_hops(m, next, d);
+        std::copy(d.begin(), d.end(), out.begin() + (size_t)l * m.n);
+        int far = next;
+        for (int i = 0; i < m.n; i++) {
+            best[i] = std::min<unsigned>(best[i], d[i]);
+            if (best[i] != 65535 && best[i] > best[far]) far = i;
+        }
+        next = far;
     }
 }
 

@@ -116,6 +116,9 @@ void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, i
 void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int A,
                                  const LocateGrid& loc, int* state, int* targ_node, float2* targ_pos,
                                  int* err);
+// requests reordered longest-first by the landmark estimate (keys: scratch, one int per request)
+void launch_order_requests(cudaStream_t s, const int4* req_in, const int* req_count, int4* req_out, int* keys,
+                           const unsigned short* lm, int L, int n);
 void launch_move_bin(cudaStream_t s, const MoverParams& p);
 void launch_cell_scan(cudaStream_t s, const MoverParams& p);
 void launch_scatter(cudaStream_t s, const MoverParams& p);
@@ -150,6 +153,9 @@ struct HostMap {
 
 // hostmap.cpp
 void build_host_map(const gmapf_node* nodes, int n, HostMap& out);
+// Hop distances from `count` landmark triangles chosen by farthest-point
+// sampling over the neighbour graph (unreachable: 65535), count * n values.
+void landmark_distances(const HostMap& m, int count, std::vector<unsigned short>& out);
 // navmesh_cdt.cpp: 0 on success, else a gmapf_status with `err` set
 int build_navmesh_cdt(const std::vector<float>& verts, const std::vector<unsigned>& edges,
                       std::vector<gmapf_node>& out, std::string& err);
@@ -178,6 +184,12 @@ struct Device {
     int dirty_cap = 0;
     // requests / counters
     int4* req = nullptr;
+    int4* req_sorted = nullptr;  // longest-first order (order_by_estimate)
+    int* req_keys = nullptr;
+    unsigned short* lm = nullptr;  // landmark hop distances, lm_count x n
+    int lm_count = 0;
+    int4* breq_sorted = nullptr;
+    int* breq_keys = nullptr;
     int* counters = nullptr;  // [req_count, mv_count, work_ctr, err, spare...]
     unsigned long long* stats = nullptr;
     // search state

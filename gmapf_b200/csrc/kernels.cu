@@ -142,6 +142,77 @@ __global__ void k_prepare_batch(const int* starts, const int* targets, int n, in
     req[k] = make_int4(-1, s, t, k);
 }
 
+// Orders requests longest-first for the persistent search: the estimate is
+// the landmark lower bound on the hop distance, max_l |d_l(s) - d_l(t)|, and
+// requests are bucketed by it in descending order.  Results do not depend
+// on the order (every request writes only its own row and agent).
+constexpr int kOrderBuckets = 1024;
+
+__global__ void __launch_bounds__(1024) k_order_requests(const int4* req_in, const int* req_count, int4* req_out,
+                                                         int* keys, const unsigned short* lm, int L, int n) {
+    __shared__ int hist[kOrderBuckets];
+    __shared__ int wmax[32];
+    __shared__ int gmax;
+    const int tid = threadIdx.x;
+    const int R = *req_count;
+    int mx = 0;
+    for (int i = tid; i < R; i += blockDim.x) {
+        const int4 q = req_in[i];
+        int est = 0;
+        if (q.y >= 0 && q.y < n && q.z >= 0 && q.z < n) {
+            for (int l = 0; l < L; l++) {
+                const int a = lm[(size_t)l * n + q.y], b = lm[(size_t)l * n + q.z];
+                const int e = (a == 65535 || b == 65535) ? 65535 : abs(a - b);
+                est = max(est, e);
+            }
+        }
+        keys[i] = est;
+        mx = max(mx, est);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((tid & 31) == 0) wmax[tid >> 5] = mx;
+    hist[tid] = 0;
+    __syncthreads();
+    if (tid < 32) {
+        int v = wmax[tid];
+        for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (tid == 0) gmax = v;
+    }
+    __syncthreads();
+    const long long den = max(1, gmax);
+    for (int i = tid; i < R; i += blockDim.x) {
+        const int b = (kOrderBuckets - 1) - (int)(((long long)keys[i] * (kOrderBuckets - 1)) / den);
+        keys[i] = b;
+        atomicAdd(hist + b, 1);
+    }
+    __syncthreads();
+    // exclusive scan of the histogram (one value per thread)
+    int v = hist[tid];
+    const int lane = tid & 31, w = tid >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wmax[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = wmax[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        wmax[lane] = s;  // inclusive warp sums
+    }
+    __syncthreads();
+    hist[tid] = x - v + (w > 0 ? wmax[w - 1] : 0);
+    __syncthreads();
+    for (int i = tid; i < R; i += blockDim.x) {
+        const int pos = atomicAdd(hist + keys[i], 1);
+        req_out[pos] = req_in[i];
+    }
+}
+
 // move (AgentsMover.h:51-71) fused with the agent-grid histogram
 __global__ void k_move_bin(MoverParams p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -376,6 +447,11 @@ void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets,
                           int4* req, int* req_count, int* work_ctr, int* err) {
     k_prepare_batch<<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(starts, targets, n, nodes, req,
                                                                    req_count, work_ctr, err);
+}
+
+void launch_order_requests(cudaStream_t s, const int4* req_in, const int* req_count, int4* req_out, int* keys,
+                           const unsigned short* lm, int L, int n) {
+    k_order_requests<<<1, 1024, 0, s>>>(req_in, req_count, req_out, keys, lm, L, n);
 }
 
 void launch_move_bin(cudaStream_t s, const MoverParams& p) {

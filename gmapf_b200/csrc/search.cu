@@ -35,10 +35,10 @@
 //     when it fits, else a 32-byte record per (slot, node) in global memory
 //     stamped with the query epoch (no clearing between queries);
 //   - records (G, parent and five further ancestors) are written once per
-//     claimed node; the path walk reads one record per six hops;
-//   - rows of newly queued nodes are prefetched into L1, so the next round's
-//     expansion usually hits L1; idle warps refill from a device work counter
-//     (persistent form) or stop (plain form).
+//     claimed node; the path walk reads one record per six hops; a node's
+//     record is read when it is expanded, in flight together with its row;
+//   - idle warps refill from a device work counter (persistent form) or
+//     stop (plain form).
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -55,10 +55,8 @@ __device__ __forceinline__ bool key_less(float fa, int ga, int ia, float fb, int
     return ia < ib;
 }
 
-// A queued node: its key (F, G<<1|dir, id) and its five nearest ancestors,
-// which become ancestors 1..5 of the nodes it claims (so expanding it reads
-// no record from global memory).
-constexpr int kEntryWords = 8;
+// A queued node: its key (F, G<<1|dir, id).
+constexpr int kEntryWords = 3;
 
 // Per-lane sorted ring in shared memory: word w of entry k of lane q at
 // [(w*C + k)*T + q].
@@ -73,44 +71,19 @@ struct Ring {
     __device__ __forceinline__ int* word(int w) const { return base + w * C * T; }
 };
 
-struct Entry {
-    float F;
-    int gd, id;
-    int a[5];
-};
-
-__device__ __forceinline__ void entry_load(const Ring& r, int k, Entry& e) {
-    e.F = __int_as_float(r.word(0)[k]);
-    e.gd = r.word(1)[k];
-    e.id = r.word(2)[k];
-#pragma unroll
-    for (int j = 0; j < 5; j++) e.a[j] = r.word(3 + j)[k];
-}
-
-__device__ __forceinline__ void entry_store(const Ring& r, int k, const Entry& e) {
-    r.word(0)[k] = __float_as_int(e.F);
-    r.word(1)[k] = e.gd;
-    r.word(2)[k] = e.id;
-#pragma unroll
-    for (int j = 0; j < 5; j++) r.word(3 + j)[k] = e.a[j];
-}
-
-// pop the minimum (element size-1; elements are kept in descending order);
-// returns the ring slot, whose ancestor words stay intact until this
-// round's pushes
-__device__ __forceinline__ int ring_pop(const Ring& r, int beg, int& size, int& gd, int& id) {
+// pop the minimum (element size-1; elements are kept in descending order)
+__device__ __forceinline__ void ring_pop(const Ring& r, int beg, int& size, int& gd, int& id) {
     const int k = r.at(beg + size - 1);
     gd = r.word(1)[k];
     id = r.word(2)[k];
     size--;
-    return k;
 }
 
 // bounded push (CuQueue.h:33-63 with the (F,G,id) order)
-__device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, const Entry& x) {
+__device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, float F, int gd, int id) {
     if (size == r.C) {
         const int k0 = r.at(beg);
-        if (!key_less(x.F, x.gd, x.id, __int_as_float(r.word(0)[k0]), r.word(1)[k0], r.word(2)[k0]))
+        if (!key_less(F, gd, id, __int_as_float(r.word(0)[k0]), r.word(1)[k0], r.word(2)[k0]))
             return;                            // not below the maximum: dropped
         beg = (beg + 1 == r.C) ? 0 : beg + 1;  // evict the maximum
         size--;
@@ -118,13 +91,19 @@ __device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, co
     int i = size - 1;
     while (i >= 0) {
         const int k = r.at(beg + i);
-        if (!key_less(__int_as_float(r.word(0)[k]), r.word(1)[k], r.word(2)[k], x.F, x.gd, x.id)) break;
-        Entry e;
-        entry_load(r, k, e);
-        entry_store(r, r.at(beg + i + 1), e);
+        const float ef = __int_as_float(r.word(0)[k]);
+        const int eg = r.word(1)[k], ei = r.word(2)[k];
+        if (!key_less(ef, eg, ei, F, gd, id)) break;
+        const int k1 = r.at(beg + i + 1);
+        r.word(0)[k1] = __float_as_int(ef);
+        r.word(1)[k1] = eg;
+        r.word(2)[k1] = ei;
         i--;
     }
-    entry_store(r, r.at(beg + i + 1), x);
+    const int k1 = r.at(beg + i + 1);
+    r.word(0)[k1] = __float_as_int(F);
+    r.word(1)[k1] = gd;
+    r.word(2)[k1] = id;
     size++;
 }
 
@@ -141,10 +120,6 @@ __device__ __forceinline__ void st_rec(Rec* r, unsigned stamp, int gd, int a0, i
                                        int a3, int a4, int a5) {
     __stcg(reinterpret_cast<int4*>(r), make_int4((int)stamp, gd, a0, a1));
     __stcg(reinterpret_cast<int4*>(r) + 1, make_int4(a2, a3, a4, a5));
-}
-
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 // 2-bit visited state: bit 0 = claimed, bit 1 = reached from the start
@@ -165,11 +140,6 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
     return ((size_t)kEntryWords * 3 * T + 3) & ~(size_t)3;
 }
 
-__device__ __forceinline__ void prefetch_row(const SearchRow* rows, int id) {
-    const char* rp = reinterpret_cast<const char*>(rows + id);
-    prefetch_l1(rp);
-    prefetch_l1(rp + sizeof(SearchRow) - 1);
-}
 
 template <int T, bool SMEMV>
 __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
@@ -219,8 +189,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
             const bool bad = start != target || start < 0 || start >= n_nodes;
             if (lane == 0) {  // bad request: not found; start == target: found, empty path
                 if (bad) atomicOr(p.err, ERR_BAD_REQUEST);
-                if (p.out_found) p.out_found[r] = bad ? 0 : 1;
-                if (p.out_len) p.out_len[r] = 0;
+                if (p.out_found) p.out_found[orow] = bad ? 0 : 1;
+                if (p.out_len) p.out_len[orow] = 0;
                 if (agent >= 0 && p.ag_state) {
                     p.ag_state[agent] = GMAPF_AGENT_IDLE;
                     p.ag_path_len[agent] = 0;
@@ -253,16 +223,10 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         int qbeg = 0, qsize = 0;  // lanes < T: this lane's queue
         if (lane < 2) {           // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
             const int node = lane == 0 ? start : target;
-            Entry e;
-            e.F = f0;
-            e.gd = lane == 0 ? 1 : 0;
-            e.id = node;
-#pragma unroll
-            for (int j = 0; j < 5; j++) e.a[j] = -1;
-            ring_push(ring, qbeg, qsize, e);
-            st_rec(rec + node, ep, e.gd, -1, -1, -1, -1, -1, -1);
-            if (SMEMV) bm_set(bm, node, e.gd);
-            prefetch_row(p.rows, node);
+            const int gd = lane == 0 ? 1 : 0;
+            ring_push(ring, qbeg, qsize, f0, gd, node);
+            st_rec(rec + node, ep, gd, -1, -1, -1, -1, -1, -1);
+            if (SMEMV) bm_set(bm, node, gd);
         }
         __syncwarp();
 
@@ -273,37 +237,54 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         for (;;) {
             rounds++;
             // lanes < T pop their minimum
-            int idu = -1, gdu = 0, uslot = 0;
-            if (lane < T && qsize > 0) uslot = ring_pop(ring, qbeg, qsize, gdu, idu);
+            int idu = -1, gdu = 0;
+            if (lane < T && qsize > 0) ring_pop(ring, qbeg, qsize, gdu, idu);
 
+            // gather: every pass's candidate data, all loads in flight together
+            int cu[NP], cgdu[NP], cn[NP];
+            float cx[NP], cy[NP];
+            bool cval[NP];
+            int4 ra[NP], rb[NP];
+            int2 cst[NP];
+#pragma unroll
+            for (int pass = 0; pass < NP; pass++) {
+                const int c = pass * 32 + lane;  // candidate order = slot * T + lane
+                const int s = c / T, qq = c - s * T;
+                cu[pass] = __shfl_sync(kFull, idu, qq & 31);
+                cgdu[pass] = __shfl_sync(kFull, gdu, qq & 31);
+                cval[pass] = c < 3 * T && cu[pass] >= 0;
+                cn[pass] = -1;
+                cx[pass] = cy[pass] = 0.f;
+                ra[pass] = make_int4(0, 0, -1, -1);
+                rb[pass] = make_int4(-1, -1, -1, -1);
+                cst[pass] = make_int2(0, 0);
+                if (cval[pass]) {
+                    const SearchRow* rw = p.rows + cu[pass];
+                    const int4 r0 = __ldg(reinterpret_cast<const int4*>(rw));
+                    const float2 cc = __ldg(reinterpret_cast<const float2*>(&rw->x0) + s);
+                    ld_rec(rec + cu[pass], ra[pass], rb[pass]);  // the popped node's ancestors
+                    cn[pass] = (s == 0) ? r0.x : (s == 1) ? r0.y : r0.z;
+                    cval[pass] = s < r0.w;
+                    cx[pass] = cc.x;
+                    cy[pass] = cc.y;
+                    if (s == 0) {
+                        expansions++;
+                        deg_sum += (unsigned)r0.w;
+                    }
+                    if (!SMEMV && cval[pass]) cst[pass] = ld_state(rec + cn[pass]);  // claims of earlier rounds
+                }
+            }
+
+            // resolve: passes in candidate order
             int nwin = 0;
             bool meet = false;
             int mu = 0, mgu = 0, mn = 0, mgn = 0, mgn_known = 0;
 #pragma unroll
             for (int pass = 0; pass < NP; pass++) {
-                const int c = pass * 32 + lane;          // candidate order = slot * T + lane
-                const int s = c / T, qq = c - s * T;
-                const int cu = __shfl_sync(kFull, idu, qq & 31);
-                const int cgdu = __shfl_sync(kFull, gdu, qq & 31);
-                const int cslot = __shfl_sync(kFull, uslot, qq & 31);
-                bool valid = c < 3 * T && cu >= 0;
-                int n = -1;
-                float nx = 0.f, ny = 0.f;
-                if (valid) {
-                    const SearchRow* rw = p.rows + cu;
-                    const int4 r0 = __ldg(reinterpret_cast<const int4*>(rw));
-                    const float2 cc = __ldg(reinterpret_cast<const float2*>(&rw->x0) + s);
-                    n = (s == 0) ? r0.x : (s == 1) ? r0.y : r0.z;
-                    valid = s < r0.w;
-                    nx = cc.x;
-                    ny = cc.y;
-                    if (s == 0) {
-                        expansions++;
-                        deg_sum += (unsigned)r0.w;
-                    }
-                }
-                const int du = cgdu & 1;
-                const int ngd = (((cgdu >> 1) + 1) << 1) | du;
+                const int n = cn[pass];
+                const bool valid = cval[pass];
+                const int du = cgdu[pass] & 1;
+                const int ngd = (((cgdu[pass] >> 1) + 1) << 1) | du;
                 bool prev = false;
                 int pgd = 0, pknown = 0;
                 if (valid) {
@@ -312,12 +293,18 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                         prev = (st & 1) != 0;
                         pgd = st >> 1;                 // side only; G read at the meet
                     } else {
-                        // sees claims of earlier passes too: their record stores are
-                        // ordered before this load by the pass's __syncwarp
-                        const int2 st = ld_state(rec + n);
-                        prev = (unsigned)st.x == ep;
-                        pgd = st.y;
+                        prev = (unsigned)cst[pass].x == ep;
+                        pgd = cst[pass].y;
                         pknown = 1;
+                        if (pass > 0 && !prev) {  // claimed by an earlier pass of this round
+                            int hit = -1;
+#pragma unroll 8
+                            for (int w = 0; w < nwin; w++) hit = (fr[6 * T + w] == n) ? w : hit;
+                            if (hit >= 0) {
+                                prev = true;
+                                pgd = fr[3 * T + hit];
+                            }
+                        }
                     }
                 }
                 const bool fresh = valid && !prev;
@@ -338,8 +325,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 const unsigned cm = __ballot_sync(kFull, conflict);
                 if (!meet && cm != 0u) {  // warp-uniform
                     const int ml = __ffs(cm) - 1;
-                    mu = __shfl_sync(kFull, cu, ml);
-                    mgu = __shfl_sync(kFull, cgdu, ml);
+                    mu = __shfl_sync(kFull, cu[pass], ml);
+                    mgu = __shfl_sync(kFull, cgdu[pass], ml);
                     mn = __shfl_sync(kFull, n, ml);
                     mgn = __shfl_sync(kFull, cgd, ml);
                     mgn_known = __shfl_sync(kFull, cknown, ml);
@@ -350,27 +337,14 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                     const int idx = nwin + __popc(wm & lt_mask);
                     const float farx = du ? ct.x : cs.x;
                     const float fary = du ? ct.y : cs.y;
-                    const float hh = dist_sqr(nx, ny, farx, fary);
+                    const float hh = dist_sqr(cx[pass], cy[pass], farx, fary);
                     const float F = GM_FADD((float)(ngd >> 1), GM_FMUL(hh, K));
-                    // ancestors 1..5 of n = the popped node's ancestors 0..4 (its queue slot)
-                    int ua[5];
-#pragma unroll
-                    for (int j = 0; j < 5; j++) ua[j] = ring.base[(3 + j) * C * T + cslot];
-                    fr[0 * 3 * T + idx] = __float_as_int(F);
-                    fr[1 * 3 * T + idx] = ngd;
-                    fr[2 * 3 * T + idx] = n;
-                    fr[3 * 3 * T + idx] = cu;
-#pragma unroll
-                    for (int j = 0; j < 4; j++) fr[(4 + j) * 3 * T + idx] = ua[j];
+                    fr[idx] = __float_as_int(F);
+                    fr[3 * T + idx] = ngd;
+                    fr[6 * T + idx] = n;
                     if (SMEMV) bm_set(bm, n, du);
-                    st_rec(rec + n, ep, ngd, cu, ua[0], ua[1], ua[2], ua[3], ua[4]);
-                    // the rows this node's expansion will read next: its neighbours'
-                    const int* gg = p.rows[cu].g + 3 * s;
-#pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        const int m = __ldg(gg + j);
-                        if (m >= 0 && m != cu) prefetch_row(p.rows, m);
-                    }
+                    // ancestors 1..5 of n = ancestors 0..4 of the popped node
+                    st_rec(rec + n, ep, ngd, cu[pass], ra[pass].z, ra[pass].w, rb[pass].x, rb[pass].y, rb[pass].z);
                 }
                 nwin += __popc(wm);
                 __syncwarp();
@@ -398,15 +372,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 ended = true;
             } else {
                 if (lane < T) {
-                    for (int i = lane; i < nwin; i += T) {
-                        Entry e;
-                        e.F = __int_as_float(fr[i]);
-                        e.gd = fr[3 * T + i];
-                        e.id = fr[2 * 3 * T + i];
-#pragma unroll
-                        for (int j = 0; j < 5; j++) e.a[j] = fr[(3 + j) * 3 * T + i];
-                        ring_push(ring, qbeg, qsize, e);
-                    }
+                    for (int i = lane; i < nwin; i += T)
+                        ring_push(ring, qbeg, qsize, __int_as_float(fr[i]), fr[3 * T + i], fr[6 * T + i]);
                 }
                 if (!__any_sync(kFull, qsize > 0)) ended = true;
                 if ((int)rounds >= p.max_rounds) {
@@ -465,8 +432,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         const unsigned ex = __reduce_add_sync(kFull, expansions);
         const unsigned ds = __reduce_add_sync(kFull, deg_sum);
         if (lane == 0) {
-            if (p.out_found) p.out_found[r] = found;
-            if (p.out_len) p.out_len[r] = L;
+            if (p.out_found) p.out_found[orow] = found;
+            if (p.out_len) p.out_len[orow] = L;
             if (agent >= 0 && p.ag_state) {
                 p.ag_state[agent] = found ? GMAPF_AGENT_MOVE : GMAPF_AGENT_IDLE;
                 p.ag_step_idx[agent] = -1;

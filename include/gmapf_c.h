@@ -86,7 +86,8 @@ typedef struct gmapf_options {
     int32_t block_threads;     /* search block size, 0 = automatic */
     int32_t autotune;          /* 1: pick threads/agent, queue capacity and block size per map at start */
     int64_t search_mem_budget; /* bytes for per-slot search records, 0 = automatic */
-    int32_t order_by_estimate; /* 1: serve long searches first (results do not depend on it) */
+    int32_t order_by_estimate; /* 1 (default): batched form serves the searches with the largest
+                                  landmark hop-distance estimate first; results do not depend on it */
     int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records */
     int32_t _reserved[4];
 } gmapf_options;

@@ -5,11 +5,12 @@ import gmapf_b200 as G
 from gmapf_b200 import scenarios as S
 
 
-def map_world(scn, T=None, Cap=None, mode=G.MODE_BATCHED, agents=4, block_threads=0, visited_mode=0):
+def map_world(scn, T=None, Cap=None, mode=G.MODE_BATCHED, agents=4, block_threads=0, visited_mode=0,
+              order=True):
     g = G.GMAPF()
     g.Init(G.make_config(agents, scn.radius, scn.speed, agents, T or scn.threads_per_agent,
                          Cap or scn.queue_capacity, scn.heuristic_k))
-    g.set_options(mode=mode, block_threads=block_threads, visited_mode=visited_mode)
+    g.set_options(mode=mode, block_threads=block_threads, visited_mode=visited_mode, order_by_estimate=order)
     S.build_map(g, scn)
     return g
 

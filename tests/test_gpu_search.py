@@ -76,6 +76,17 @@ def test_plain_equals_batched(oracle_mod, vm):
     assert np.array_equal(fb, fp) and np.array_equal(lb, lp) and np.array_equal(pb, pp)
 
 
+def test_longest_first_order_does_not_change_results(oracle_mod):
+    scn = S.cfg3(cells=32)
+    go = map_world(scn, T=8, Cap=16, order=True)
+    gu = map_world(scn, T=8, Cap=16, order=False)
+    s, t = random_queries(go, scn, 3000, seed=15)
+    a = go.search_batch(s, t, go.node_count)
+    b = gu.search_batch(s, t, gu.node_count)
+    assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
+    assert a[3]["expansions"] == b[3]["expansions"]
+
+
 @pytest.mark.parametrize("bt", [32, 64, 256])
 def test_block_shape_does_not_change_results(oracle_mod, bt):
     scn = S.cfg2()
