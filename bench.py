@@ -161,6 +161,19 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_traffic(cells: int, T: int, C: int, queries_per_step: float):
+    """DRAM bytes per search launch from the committed ncu capture
+    (profiles/search_traffic.json, per query, scaled to this frame's
+    queries), or None when no capture matches this workload."""
+    p = ROOT / "profiles" / "search_traffic.json"
+    if not p.exists():
+        return None, None
+    d = json.loads(p.read_text()).get(f"maze{cells}_T{T}_C{C}")
+    if not d:
+        return None, None
+    return d["bytes_per_query"] * queries_per_step, d["source"]
+
+
 def algorithmic_bytes(st: dict, n_nodes: int) -> float:
     """Search bytes by the fixed per-unit definitions: per expansion 12 B of
     adjacency plus 24 B per neighbour (centroid, visited word, record); per
@@ -292,6 +305,7 @@ def bench_b200(args):
     ab = [algorithmic_bytes(s, n_nodes) for s in dstats]
     achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
+    traffic, traffic_src = measured_traffic(args.cells, T, C, queries / max(1, K))
 
     # plain per-agent form on the same frames
     plain = None
@@ -352,7 +366,8 @@ def bench_b200(args):
             "batched_over_plain": (e2e_value / plain["value"]) if plain else None,
             "roofline": {"bound": "hbm", "kernel": "k_search", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "search_ms_per_step": statistics.mean(search_ms),
+                         "traffic": traffic, "traffic_source": traffic_src,
+                         "search_ms_per_step": statistics.mean(search_ms),
                          "algorithmic_bytes_per_step": statistics.mean(ab)},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "path queries/s", "h2d_bytes_per_step": 16 * A + 4,

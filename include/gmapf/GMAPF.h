@@ -1,0 +1,153 @@
+// gmapf/GMAPF.h -- header-only C++ front-end of the B200 G-MAPF library with
+// the reference's public names and signatures (rosdvp/gmapf
+// include/gmapf/GMAPF.h:30-98, Config.h:5-18, Agent.h:7-12,
+// misc/V2Float.h:12-16, misc/CuNodesMap.h:14-21), over the C ABI in
+// gmapf_c.h.  Code written against the reference compiles against this
+// header and links with libgmapf_b200.so.
+//
+// Errors: the reference throws std::exception("message") (an MSVC extension,
+// src/GMAPF.cu:75-329); this wrapper throws gmapf::Error, a
+// std::runtime_error carrying the C status, so `catch (std::exception&)`
+// keeps working and what() returns the message.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../gmapf_c.h"
+
+namespace gmapf {
+
+// include/gmapf/misc/V2Float.h:12-16 (layout; arithmetic is not needed by the API)
+struct V2Float {
+    float X = 0;
+    float Y = 0;
+    V2Float() = default;
+    V2Float(float x, float y) : X(x), Y(y) {}
+};
+
+// include/gmapf/Agent.h:7-12
+enum class EAgentState { Idle = 0, Search = 1, Move = 2 };
+
+// include/gmapf/Config.h:5-18
+struct Config {
+    int AgentsMaxCount;
+    float AgentRadius;
+    float AgentSpeed;
+    int PathFinderParallelAgents;
+    int PathFinderThreadsPerAgents;
+    int PathFinderQueueCapacity;
+    float PathFinderHeuristicK;
+    bool IsDebug = false;
+    bool IsProfiler = false;
+};
+
+// include/gmapf/misc/CuNodesMap.h:14-21 (CuNodesMap::Node)
+class CuNodesMap {
+public:
+    constexpr static int INVALID = -1;
+    constexpr static int NEIBS_MAX_COUNT = 3;
+    struct alignas(16) Node {
+        V2Float P1;
+        V2Float P2;
+        V2Float P3;
+        V2Float PCenter;
+        int NeibsIdx[NEIBS_MAX_COUNT];
+    };
+};
+static_assert(sizeof(CuNodesMap::Node) == sizeof(gmapf_node), "Node layout");
+static_assert(sizeof(V2Float) == sizeof(gmapf_v2), "V2Float layout");
+
+class Error : public std::runtime_error {
+public:
+    Error(gmapf_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+    gmapf_status status;
+};
+
+class GMAPF {
+public:
+    GMAPF() {
+        check(gmapf_create(&_ctx));
+    }
+    GMAPF(const GMAPF&) = delete;
+    GMAPF(GMAPF&&) = delete;
+    GMAPF& operator=(GMAPF&) = delete;
+    GMAPF& operator=(GMAPF&&) = delete;
+    ~GMAPF() { gmapf_destroy(_ctx); }  // waits for a running step, frees everything
+
+    void Init(const Config& c) {
+        gmapf_config cc{};
+        cc.AgentsMaxCount = c.AgentsMaxCount;
+        cc.AgentRadius = c.AgentRadius;
+        cc.AgentSpeed = c.AgentSpeed;
+        cc.PathFinderParallelAgents = c.PathFinderParallelAgents;
+        cc.PathFinderThreadsPerAgents = c.PathFinderThreadsPerAgents;
+        cc.PathFinderQueueCapacity = c.PathFinderQueueCapacity;
+        cc.PathFinderHeuristicK = c.PathFinderHeuristicK;
+        cc.IsDebug = c.IsDebug ? 1 : 0;
+        cc.IsProfiler = c.IsProfiler ? 1 : 0;
+        check(gmapf_init(_ctx, &cc));
+    }
+    void ManualStart() { check(gmapf_manual_start(_ctx)); }
+
+    int AddAgent(const V2Float& currPos) {
+        int32_t id = -1;
+        check(gmapf_add_agent(_ctx, currPos.X, currPos.Y, &id));
+        return id;
+    }
+    void SetAgentTargPos(int agentId, const V2Float& targPos) {
+        check(gmapf_set_agent_targ_pos(_ctx, agentId, targPos.X, targPos.Y));
+    }
+    // README.md:78 spelling
+    void SetAgentTargetPos(int agentId, const V2Float& targPos) { SetAgentTargPos(agentId, targPos); }
+
+    void FillMapStart(const V2Float& mapSize) { check(gmapf_fill_map_start(_ctx, mapSize.X, mapSize.Y)); }
+    // README.md:66 calls it with two numbers
+    void FillMapStart(float sizeX, float sizeY) { check(gmapf_fill_map_start(_ctx, sizeX, sizeY)); }
+    void FillMapObstacle(const std::vector<V2Float>& vertices) {
+        check(gmapf_fill_map_obstacle(_ctx, reinterpret_cast<const gmapf_v2*>(vertices.data()),
+                                      (int32_t)vertices.size()));
+    }
+    void FillMapEnd() { check(gmapf_fill_map_end(_ctx)); }
+    void FillMapManually(const std::vector<CuNodesMap::Node>& nodes) {
+        std::vector<gmapf_node> n(nodes.size());
+        for (size_t i = 0; i < nodes.size(); i++) {
+            n[i].P1 = {nodes[i].P1.X, nodes[i].P1.Y};
+            n[i].P2 = {nodes[i].P2.X, nodes[i].P2.Y};
+            n[i].P3 = {nodes[i].P3.X, nodes[i].P3.Y};
+            n[i].PCenter = {nodes[i].PCenter.X, nodes[i].PCenter.Y};
+            for (int k = 0; k < 3; k++) n[i].NeibsIdx[k] = nodes[i].NeibsIdx[k];
+            n[i]._pad = 0;
+        }
+        check(gmapf_fill_map_manually(_ctx, n.data(), (int32_t)n.size()));
+    }
+
+    void AsyncStep(float deltaTime) { check(gmapf_async_step(_ctx, deltaTime)); }
+    void WaitStepEnd() { check(gmapf_wait_step_end(_ctx)); }
+
+    // a reference into the host mirror, refreshed by WaitStepEnd (src/GMAPF.cu:316-319)
+    const V2Float& GetAgentPos(int agentId) {
+        if (agentId < 0 || agentId >= gmapf_agent_count(_ctx)) throw Error(GMAPF_E_INVALID_ARG, "agent id out of range");
+        return reinterpret_cast<const V2Float*>(gmapf_agent_pos_view(_ctx))[agentId];
+    }
+    EAgentState GetAgentState(int agentId) {
+        int32_t s = 0;
+        check(gmapf_get_agent_state(_ctx, agentId, &s));
+        return static_cast<EAgentState>(s);
+    }
+
+    void ProfilerDump() const { check(gmapf_profiler_dump(_ctx)); }
+
+    // the C context, for the extensions in gmapf_c.h
+    gmapf_ctx* handle() const { return _ctx; }
+
+private:
+    gmapf_ctx* _ctx = nullptr;
+    static void check(gmapf_status s) {
+        if (s != GMAPF_OK) throw Error(s, std::string("[gmapf] ") + gmapf_last_error());
+    }
+};
+
+}  // namespace gmapf
