@@ -71,17 +71,11 @@ struct Ring {
     __device__ __forceinline__ int* word(int w) const { return base + w * C * T; }
 };
 
-// pop the minimum (element size-1; elements are kept in descending order)
-__device__ __forceinline__ void ring_pop(const Ring& r, int beg, int& size, int& gd, int& id) {
-    const int k = r.at(beg + size - 1);
-    gd = r.word(1)[k];
-    id = r.word(2)[k];
-    size--;
-}
-
-// bounded push (CuQueue.h:33-63 with the (F,G,id) order)
-__device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, float F, int gd, int id) {
-    if (size == r.C) {
+// bounded push (CuQueue.h:33-63 with the (F,G,id) order) into a ring holding
+// at most cap entries, kept in descending order (minimum at the tail)
+__device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, int cap, float F, int gd, int id) {
+    if (cap <= 0) return;
+    if (size == cap) {
         const int k0 = r.at(beg);
         if (!key_less(F, gd, id, __int_as_float(r.word(0)[k0]), r.word(1)[k0], r.word(2)[k0]))
             return;                            // not below the maximum: dropped
@@ -143,7 +137,6 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
 
 template <int T, bool SMEMV>
 __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
-    constexpr int NP = (3 * T + 31) / 32;  // candidate passes per round
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;                 // warp in block
@@ -220,14 +213,30 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         const float2 cs = p.cen[start];
         const float2 ct = p.cen[target];
         const float f0 = GM_FMUL(dist_sqr(cs.x, cs.y, ct.x, ct.y), K);
-        int qbeg = 0, qsize = 0;  // lanes < T: this lane's queue
-        if (lane < 2) {           // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
+        // Lane q's queue (lanes < T) is kept as: the node selected for the
+        // coming round (uid/ugd, -1 if none), the ring in shared memory with its
+        // minimum cached in registers (tF/tgd/tid), and up to three received
+        // items waiting to be inserted (px*).  Pushing a round's items and then
+        // popping the minimum equals selecting the minimum of (ring ∪ items)
+        // first and inserting the rest with capacity C-1, so the insertion can
+        // run while the next round's loads are in flight.
+        int qbeg = 0, qsize = 0;
+        int uid = -1, ugd = 0;
+        float tF = 0.f;
+        int tgd = 0, tid = -1;
+        bool pop_tail = false;
+        bool pv[3] = {false, false, false};  // received items waiting for insertion
+        float pxF[3] = {0.f, 0.f, 0.f};
+        int pxg[3] = {0, 0, 0}, pxi[3] = {0, 0, 0};
+        if (lane < 2) {  // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
             const int node = lane == 0 ? start : target;
             const int gd = lane == 0 ? 1 : 0;
-            ring_push(ring, qbeg, qsize, f0, gd, node);
+            uid = node;
+            ugd = gd;
             st_rec(rec + node, ep, gd, -1, -1, -1, -1, -1, -1);
             if (SMEMV) bm_set(bm, node, gd);
         }
+        (void)f0;  // the seeds' F never takes part in a comparison: each seed is alone in its queue
         __syncwarp();
 
         unsigned expansions = 0, deg_sum = 0, claims = 2, rounds = 0;
@@ -236,55 +245,21 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         // ------------------------------------------------------------ rounds
         for (;;) {
             rounds++;
-            // lanes < T pop their minimum
-            int idu = -1, gdu = 0;
-            if (lane < T && qsize > 0) ring_pop(ring, qbeg, qsize, gdu, idu);
+            // lanes < T expand the node selected at the end of the previous round
+            const int idu = (lane < T) ? uid : -1;
+            const int gdu = ugd;
 
-            // gather: every pass's candidate data, all loads in flight together
-            int cu[NP], cgdu[NP], cn[NP];
-            float cx[NP], cy[NP];
-            bool cval[NP];
-            int4 ra[NP], rb[NP];
-            int2 cst[NP];
-#pragma unroll
-            for (int pass = 0; pass < NP; pass++) {
-                const int c = pass * 32 + lane;  // candidate order = slot * T + lane
-                const int s = c / T, qq = c - s * T;
-                cu[pass] = __shfl_sync(kFull, idu, qq & 31);
-                cgdu[pass] = __shfl_sync(kFull, gdu, qq & 31);
-                cval[pass] = c < 3 * T && cu[pass] >= 0;
-                cn[pass] = -1;
-                cx[pass] = cy[pass] = 0.f;
-                ra[pass] = make_int4(0, 0, -1, -1);
-                rb[pass] = make_int4(-1, -1, -1, -1);
-                cst[pass] = make_int2(0, 0);
-                if (cval[pass]) {
-                    const SearchRow* rw = p.rows + cu[pass];
-                    const int4 r0 = __ldg(reinterpret_cast<const int4*>(rw));
-                    const float2 cc = __ldg(reinterpret_cast<const float2*>(&rw->x0) + s);
-                    ld_rec(rec + cu[pass], ra[pass], rb[pass]);  // the popped node's ancestors
-                    cn[pass] = (s == 0) ? r0.x : (s == 1) ? r0.y : r0.z;
-                    cval[pass] = s < r0.w;
-                    cx[pass] = cc.x;
-                    cy[pass] = cc.y;
-                    if (s == 0) {
-                        expansions++;
-                        deg_sum += (unsigned)r0.w;
-                    }
-                    if (!SMEMV && cval[pass]) cst[pass] = ld_state(rec + cn[pass]);  // claims of earlier rounds
-                }
-            }
-
-            // resolve: passes in candidate order
             int nwin = 0;
             bool meet = false;
             int mu = 0, mgu = 0, mn = 0, mgn = 0, mgn_known = 0;
-#pragma unroll
-            for (int pass = 0; pass < NP; pass++) {
-                const int n = cn[pass];
-                const bool valid = cval[pass];
-                const int du = cgdu[pass] & 1;
-                const int ngd = (((cgdu[pass] >> 1) + 1) << 1) | du;
+
+            // One claim pass over up to 32 candidates, in candidate order by
+            // thread index: visited state, the lowest fresh thread of a node
+            // claims it, the first conflicting thread is the meeting pair.
+            auto resolve = [&](bool valid, int cu, int cgdu, int n, float cx, float cy, const int4& ra,
+                               const int4& rb, int2 cst, bool later_pass) {
+                const int du = cgdu & 1;
+                const int ngd = (((cgdu >> 1) + 1) << 1) | du;
                 bool prev = false;
                 int pgd = 0, pknown = 0;
                 if (valid) {
@@ -293,12 +268,11 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                         prev = (st & 1) != 0;
                         pgd = st >> 1;                 // side only; G read at the meet
                     } else {
-                        prev = (unsigned)cst[pass].x == ep;
-                        pgd = cst[pass].y;
+                        prev = (unsigned)cst.x == ep;
+                        pgd = cst.y;
                         pknown = 1;
-                        if (pass > 0 && !prev) {  // claimed by an earlier pass of this round
+                        if (later_pass && !prev) {  // claimed by an earlier pass of this round
                             int hit = -1;
-#pragma unroll 8
                             for (int w = 0; w < nwin; w++) hit = (fr[6 * T + w] == n) ? w : hit;
                             if (hit >= 0) {
                                 prev = true;
@@ -325,8 +299,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 const unsigned cm = __ballot_sync(kFull, conflict);
                 if (!meet && cm != 0u) {  // warp-uniform
                     const int ml = __ffs(cm) - 1;
-                    mu = __shfl_sync(kFull, cu[pass], ml);
-                    mgu = __shfl_sync(kFull, cgdu[pass], ml);
+                    mu = __shfl_sync(kFull, cu, ml);
+                    mgu = __shfl_sync(kFull, cgdu, ml);
                     mn = __shfl_sync(kFull, n, ml);
                     mgn = __shfl_sync(kFull, cgd, ml);
                     mgn_known = __shfl_sync(kFull, cknown, ml);
@@ -337,17 +311,104 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                     const int idx = nwin + __popc(wm & lt_mask);
                     const float farx = du ? ct.x : cs.x;
                     const float fary = du ? ct.y : cs.y;
-                    const float hh = dist_sqr(cx[pass], cy[pass], farx, fary);
+                    const float hh = dist_sqr(cx, cy, farx, fary);
                     const float F = GM_FADD((float)(ngd >> 1), GM_FMUL(hh, K));
                     fr[idx] = __float_as_int(F);
                     fr[3 * T + idx] = ngd;
                     fr[6 * T + idx] = n;
                     if (SMEMV) bm_set(bm, n, du);
                     // ancestors 1..5 of n = ancestors 0..4 of the popped node
-                    st_rec(rec + n, ep, ngd, cu[pass], ra[pass].z, ra[pass].w, rb[pass].x, rb[pass].y, rb[pass].z);
+                    st_rec(rec + n, ep, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
                 }
                 nwin += __popc(wm);
                 __syncwarp();
+            };
+
+            // deferred queue work of the previous round, placed where the loads
+            // issued before it are still in flight
+            auto deferred_queue_work = [&]() {
+                if (lane < T) {
+                    if (pop_tail) qsize--;
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        if (pv[j]) ring_push(ring, qbeg, qsize, C - 1, pxF[j], pxg[j], pxi[j]);
+                    if (qsize > 0) {
+                        const int k = ring.at(qbeg + qsize - 1);
+                        tF = __int_as_float(ring.word(0)[k]);
+                        tgd = ring.word(1)[k];
+                        tid = ring.word(2)[k];
+                    }
+                }
+            };
+
+            if constexpr (T <= 8) {
+                // one pass: thread c = slot*T + lane handles candidate c directly
+                const int c = lane, sl = c / T, qq = c - sl * T;
+                const int cu = __shfl_sync(kFull, idu, qq & 31);
+                const int cgdu = __shfl_sync(kFull, gdu, qq & 31);
+                bool valid = c < 3 * T && cu >= 0;
+                int n = -1;
+                float cx = 0.f, cy = 0.f;
+                int4 ra = make_int4(0, 0, -1, -1), rb = make_int4(-1, -1, -1, -1);
+                int2 cst = make_int2(0, 0);
+                if (valid) {
+                    const SearchRow* rw = p.rows + cu;
+                    const int4 r0 = __ldg(reinterpret_cast<const int4*>(rw));
+                    const float2 cc = __ldg(reinterpret_cast<const float2*>(&rw->x0) + sl);
+                    ld_rec(rec + cu, ra, rb);  // the popped node's ancestors
+                    n = (sl == 0) ? r0.x : (sl == 1) ? r0.y : r0.z;
+                    valid = sl < r0.w;
+                    cx = cc.x;
+                    cy = cc.y;
+                    if (sl == 0) {
+                        expansions++;
+                        deg_sum += (unsigned)r0.w;
+                    }
+                    if (!SMEMV && valid) cst = ld_state(rec + n);  // claims of earlier rounds
+                }
+                deferred_queue_work();
+                resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, false);
+            } else {
+                // compacted candidates: slot-major (slot 0 of every expanding lane,
+                // then slot 1, then slot 2) -- usually one pass of at most 32
+                int4 r0 = make_int4(-1, -1, -1, 0);
+                if (idu >= 0) r0 = __ldg(reinterpret_cast<const int4*>(p.rows + idu));
+                deferred_queue_work();
+                const unsigned b0 = __ballot_sync(kFull, idu >= 0 && r0.w > 0);
+                const unsigned b1 = __ballot_sync(kFull, idu >= 0 && r0.w > 1);
+                const unsigned b2 = __ballot_sync(kFull, idu >= 0 && r0.w > 2);
+                if (idu >= 0) {
+                    expansions++;
+                    deg_sum += (unsigned)r0.w;
+                }
+                const int n0 = __popc(b0), n1 = __popc(b1), total = n0 + n1 + __popc(b2);
+                for (int base = 0; base < total; base += 32) {  // warp-uniform
+                    const int t = base + lane;
+                    const int sl = t < n0 ? 0 : (t < n0 + n1 ? 1 : 2);
+                    const unsigned bm_s = sl == 0 ? b0 : (sl == 1 ? b1 : b2);
+                    const int rank = t - (sl == 0 ? 0 : (sl == 1 ? n0 : n0 + n1));
+                    // the lane holding the (rank+1)-th set bit of this slot's ballot
+                    const int qq = t < total ? (int)(__fns(bm_s, 0, rank + 1) & 31u) : 0;
+                    const int cu = __shfl_sync(kFull, idu, qq);
+                    const int cgdu = __shfl_sync(kFull, gdu, qq);
+                    const int na = __shfl_sync(kFull, r0.x, qq);
+                    const int nb = __shfl_sync(kFull, r0.y, qq);
+                    const int nc = __shfl_sync(kFull, r0.z, qq);
+                    int n = sl == 0 ? na : (sl == 1 ? nb : nc);
+                    const bool valid = t < total && cu >= 0 && cu < n_nodes && n >= 0 && n < n_nodes;
+                    if (!valid) n = -1;
+                    float cx = 0.f, cy = 0.f;
+                    int4 ra = make_int4(0, 0, -1, -1), rb = make_int4(-1, -1, -1, -1);
+                    int2 cst = make_int2(0, 0);
+                    if (valid) {
+                        const float2 cc = __ldg(reinterpret_cast<const float2*>(&p.rows[cu].x0) + sl);
+                        ld_rec(rec + cu, ra, rb);
+                        cx = cc.x;
+                        cy = cc.y;
+                        if (!SMEMV) cst = ld_state(rec + n);
+                    }
+                    resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, base > 0);
+                }
             }
             claims += (unsigned)nwin;
             bool ended = false;
@@ -371,11 +432,35 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 found = 1;
                 ended = true;
             } else {
-                if (lane < T) {
-                    for (int i = lane; i < nwin; i += T)
-                        ring_push(ring, qbeg, qsize, __int_as_float(fr[i]), fr[3 * T + i], fr[6 * T + i]);
+                // frontier item i goes to queue i mod T (items lane, lane+T, lane+2T);
+                // select the next pop in registers
+                int best = -1;  // -1: the ring's minimum; 0..2: a received item
+                bool have = lane < T && qsize > 0;
+                float bF = tF;
+                int bg = tgd, bi = tid;
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    const int i = lane + j * T;
+                    pv[j] = lane < T && i < nwin;
+                    if (pv[j]) {
+                        pxF[j] = __int_as_float(fr[i]);
+                        pxg[j] = fr[3 * T + i];
+                        pxi[j] = fr[6 * T + i];
+                        if (!have || key_less(pxF[j], pxg[j], pxi[j], bF, bg, bi)) {
+                            best = j;
+                            have = true;
+                            bF = pxF[j];
+                            bg = pxg[j];
+                            bi = pxi[j];
+                        }
+                    }
                 }
-                if (!__any_sync(kFull, qsize > 0)) ended = true;
+                uid = have ? bi : -1;
+                ugd = bg;
+                pop_tail = have && best < 0;  // otherwise the ring is untouched by the pop
+#pragma unroll
+                for (int j = 0; j < 3; j++) pv[j] = pv[j] && j != best;  // the rest waits for insertion
+                if (!__any_sync(kFull, uid >= 0)) ended = true;
                 if ((int)rounds >= p.max_rounds) {
                     if (lane == 0) atomicOr(p.err, ERR_ROUNDS);
                     ended = true;
