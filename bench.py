@@ -184,10 +184,10 @@ def algorithmic_bytes(st: dict, n_nodes: int) -> float:
 
 # --------------------------------------------------------------- b200 arm --
 
-def make_scene(cells, seed, T, C, mode, agents, profiler=True):
+def make_scene(cells, seed, T, C, mode, agents, profiler=True, autotune=False):
     from gmapf_b200 import scenarios as S
     scn = S.cfg3(cells=cells, seed=seed, agents=agents, threads_per_agent=T, queue_capacity=C)
-    g, starts, rng = S.make_world(scn, mode=mode, profiler=profiler)
+    g, starts, rng = S.make_world(scn, mode=mode, profiler=profiler, autotune=autotune)
     g.ManualStart()
     return scn, g, rng
 
@@ -274,9 +274,11 @@ def bench_b200(args):
     A = args.agents
     T, C = args.threads_per_agent, args.queue_capacity
     seed = 3 + rank
-    scn, g, rng = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A)
+    autotune = not args.no_autotune
+    scn, g, rng = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A, autotune=autotune)
     n_nodes = g.node_count
     shape = g.search_shape()
+    Tb, Cb = shape["T"], shape["C"]  # the batched form's shape (autotuned per map)
     K, W = args.steps, args.warmup
     sets = target_sets(g, scn, rng, W + K, A)
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > L2
@@ -305,7 +307,18 @@ def bench_b200(args):
     ab = [algorithmic_bytes(s, n_nodes) for s in dstats]
     achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic, traffic_src = measured_traffic(args.cells, T, C, queries / max(1, K))
+    traffic, traffic_src = measured_traffic(args.cells, Tb, Cb, queries / max(1, K))
+
+    # batched form at the Config's own shape (same arithmetic as the plain form)
+    fixed = None
+    if autotune and (Tb, Cb) != (T, C) and not args.no_plain:
+        scn_f, gf, rng_f = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A)
+        msf, stf, _ = run_frames_device(gf, sets, W, K, torch, flush)
+        fixed = {"threads_per_agent": T, "queue_capacity": C, "unit": "path queries/s",
+                 "value": sum(s["requests"] for s in stf) / (sum(msf) / 1e3),
+                 "device_ms_per_step": {"mean": statistics.mean(msf), "p99": pct(msf, 99)},
+                 "found_rate": sum(s["found"] for s in stf) / max(1, sum(s["requests"] for s in stf))}
+        gf.close()
 
     # plain per-agent form on the same frames
     plain = None
@@ -319,17 +332,19 @@ def bench_b200(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        cpu = cpu_baseline(g, scn, sets, T, C, args.cpu_sample, os.cpu_count() or 1)
+        cpu = cpu_baseline(g, scn, sets, Tb, Cb, args.cpu_sample, os.cpu_count() or 1)
 
     # secondary workload: the 64x64-cell maze of the configuration text
     secondary = None
     if args.secondary_cells and args.secondary_cells != args.cells and rank == 0:
-        scn2, g2, rng2 = make_scene(args.secondary_cells, 3, T, C, G.MODE_BATCHED, A)
+        scn2, g2, rng2 = make_scene(args.secondary_cells, 3, T, C, G.MODE_BATCHED, A, autotune=autotune)
+        sh2 = g2.search_shape()
         sets2 = target_sets(g2, scn2, rng2, W + K, A)
         ms2, st2, _ = run_frames_device(g2, sets2, W, K, torch, flush)
         wall2, _ = run_frames_host(g2, target_sets(g2, scn2, rng2, W + K, A), W, K)
         secondary = {"workload": f"maze {args.secondary_cells}x{args.secondary_cells} cells",
-                     "triangles": g2.node_count,
+                     "triangles": g2.node_count, "threads_per_agent": sh2["T"],
+                     "queue_capacity": sh2["C"], "block_threads": sh2["block_threads"],
                      "value": sum(s["requests"] for s in st2) / (sum(ms2) / 1e3),
                      "e2e_value": A * K / (sum(wall2) / 1e3), "p99_step_ms": pct(wall2, 99),
                      "p50_step_ms": pct(wall2, 50), "ms_per_step_device": statistics.mean(ms2)}
@@ -352,7 +367,9 @@ def bench_b200(args):
             "data": "synthetic: seeded randomized-DFS maze, uniform free-space starts and targets",
             "config": {"workload": f"maze {args.cells}x{args.cells} cells on 4000x4000, {A} agents, all "
                                    f"retargeted every frame", "triangles": n_nodes, "agents": A,
-                       "threads_per_agent": T, "queue_capacity": C, "block_threads": shape["block_threads"],
+                       "threads_per_agent": Tb, "queue_capacity": Cb, "block_threads": shape["block_threads"],
+                       "shape_source": "autotuned per map" if autotune else "Config",
+                       "config_threads_per_agent": T, "config_queue_capacity": C,
                        "visited_mode": "shared-memory bitmap" if shape["visited_mode"] == 1 else "global records",
                        "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",
                        "l2": "flushed between frames (256 MB write); per-frame search records exceed L2",
@@ -363,6 +380,7 @@ def bench_b200(args):
             "found_rate": st_sum["found"] / max(1, st_sum["requests"]),
             "expansions_per_s": st_sum["expansions"] / (sum(ms) / 1e3),
             "plain": plain,
+            "batched_config_shape": fixed,
             "batched_over_plain": (e2e_value / plain["value"]) if plain else None,
             "roofline": {"bound": "hbm", "kernel": "k_search", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
@@ -442,6 +460,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=2048)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="batched form at the Config's T and C")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "internal.h"
@@ -50,7 +51,10 @@ int dalloc(Context& c, T** p, size_t count, std::string& err) {
         return e == cudaErrorMemoryAllocation ? GMAPF_E_CAPACITY : GMAPF_E_CUDA;
     }
     c.dev.allocs.push_back((void*)*p);
+    // cudaMemset runs on the legacy stream, which the library's non-blocking
+    // streams do not wait for: finish it before any kernel can touch the buffer
     e = cudaMemset(*p, 0, bytes);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         err = std::string("cudaMemset failed: ") + cudaGetErrorString(e);
         return GMAPF_E_CUDA;
@@ -169,12 +173,14 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     int best_bt = 0;
     bool best_smem = false;
     long long best_slots = 0;
+    const int want_vm = c.opt.visited_mode ? c.opt.visited_mode : c.tuned_vm;
+    const int want_bt = c.opt.block_threads ? c.opt.block_threads : c.tuned_bt;
     for (int vm = 1; vm <= 2; vm++) {
-        if (c.opt.visited_mode != 0 && c.opt.visited_mode != vm) continue;
+        if (want_vm != 0 && want_vm != vm) continue;
         const bool smem = vm == 1;
         const int bts[4] = {128, 64, 32, 256};
         for (int bt : bts) {
-            if (c.opt.block_threads != 0 && bt != c.opt.block_threads) continue;
+            if (want_bt != 0 && bt != want_bt) continue;
             if (bt % c.T) continue;
             const int per_sm = search_max_blocks_per_sm(c.T, c.C, bt, smem, d.bm_words);
             if (per_sm <= 0) continue;
@@ -569,7 +575,8 @@ int device_wait_step(Context& c, std::string& err) {
     const int e = c.h_small[CT_ERR];
     const int et = c.h_small[CT_ERR_TARGETS];
     if (et != 0) {  // from device-resident retargets enqueued before this step
-        CK(cudaMemset(d.counters + CT_ERR_TARGETS, 0, sizeof(int)));
+        CK(cudaMemsetAsync(d.counters + CT_ERR_TARGETS, 0, sizeof(int), d.stream));
+        CK(cudaStreamSynchronize(d.stream));
         err = "device-resident retarget rejected (agent id out of range or position in no triangle)";
         return GMAPF_E_DEVICE;
     }
@@ -737,10 +744,122 @@ int device_reconfigure_search(Context& c, std::string& err) {
     return alloc_search_state(c, err);
 }
 
+// Per-map autotuner (batched form): threads per agent T, queue capacity C,
+// visited-state placement and block size.  T and C are parameters of the
+// method itself (README.md:98-101: "picked empirically"), so the tuner keeps
+// only shapes whose found rate on the sample is within 0.1% of the best one
+// and, among those, takes the fastest.  The sample is seeded uniform triangle
+// pairs of this navmesh; block size follows from pick_slots for each
+// (T, C, placement).
 int device_autotune(Context& c, std::string& err) {
-    (void)c;
-    (void)err;
-    return GMAPF_OK;
+    Device& d = c.dev;
+    const int n = c.map.n;
+    if (n < 2) return GMAPF_OK;
+    // the sample is as large as a frame's request batch (2,048..8,192), so that
+    // the tuner weighs throughput as a frame does, with its path rows kept
+    // under 8 GB and a quarter of the free memory
+    size_t freeb = 0, totalb = 0;
+    CK(cudaMemGetInfo(&freeb, &totalb));
+    const double row_cap = std::min(8e9, 0.25 * (double)freeb);
+    int Q = std::min(8192, std::max(2048, c.cfg.PathFinderParallelAgents));
+    while (Q > 128 && (double)Q * n * 4 > row_cap) Q /= 2;
+    std::vector<int> hs(Q), ht(Q);
+    unsigned long long x = 0x9e3779b97f4a7c15ull;
+    for (int i = 0; i < Q; i++) {
+        x = x * 6364136223846793005ull + 1442695040888963407ull;
+        hs[i] = (int)((x >> 33) % (unsigned long long)n);
+        x = x * 6364136223846793005ull + 1442695040888963407ull;
+        ht[i] = (int)((x >> 33) % (unsigned long long)n);
+    }
+    int *ds = nullptr, *dt = nullptr, *dfound = nullptr, *dlens = nullptr, *dpaths = nullptr;
+    auto release = [&]() {
+        for (int* p : {ds, dt, dfound, dlens, dpaths})
+            if (p) cudaFree(p);
+    };
+    if (cudaMalloc(&ds, 4 * Q) != cudaSuccess || cudaMalloc(&dt, 4 * Q) != cudaSuccess ||
+        cudaMalloc(&dfound, 4 * Q) != cudaSuccess || cudaMalloc(&dlens, 4 * Q) != cudaSuccess ||
+        cudaMalloc(&dpaths, (size_t)4 * Q * n) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        err = "autotune: cannot allocate the sample buffers";
+        return GMAPF_E_CAPACITY;
+    }
+    if (cudaMemcpyAsync(ds, hs.data(), 4 * Q, cudaMemcpyHostToDevice, d.stream) != cudaSuccess ||
+        cudaMemcpyAsync(dt, ht.data(), 4 * Q, cudaMemcpyHostToDevice, d.stream) != cudaSuccess ||
+        cudaStreamSynchronize(d.stream) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        err = "autotune: cannot upload the sample";
+        return GMAPF_E_CUDA;
+    }
+
+    struct Trial {
+        int T, C, vm, bt;
+        float ms;
+        long long found;
+    };
+    std::vector<Trial> trials;
+    const int T0 = c.T, C0 = c.C;
+    // one trial: the sample twice, the faster time kept (a shape that is
+    // already three times slower than the best so far is not repeated)
+    float best_so_far = 1e30f;
+    auto trial = [&](int T, int C, int vm, int bt) {
+        c.T = T;
+        c.C = C;
+        c.tuned_vm = vm;
+        c.tuned_bt = bt;
+        std::string e2;
+        if (device_reconfigure_search(c, e2) != GMAPF_OK) return;  // shape does not fit
+        gmapf_step_stats st{};
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            if (device_search_batch(c, ds, dt, Q, dfound, dlens, dpaths, n, &st, e2) != GMAPF_OK) return;
+            ms = std::min(ms, c.last_search_ms);
+            if (ms > 3.0f * best_so_far) break;
+        }
+        best_so_far = std::min(best_so_far, ms);
+        trials.push_back({T, C, c.dev.smemv ? 1 : 2, c.block_threads, ms, (long long)st.found});
+    };
+    // stage 1: threads per agent x queue capacity x visited placement, block
+    // size by occupancy
+    std::vector<int> Ts = {32, 16, 8, 4, 2}, Cs = {8, 16, 32, 64, 128, 256};  // likely-fast shapes first
+    if (std::find(Cs.begin(), Cs.end(), C0) == Cs.end()) Cs.push_back(C0);
+    for (int T : Ts)
+        for (int C : Cs)
+            for (int vm = 1; vm <= 2; vm++)
+                if (c.opt.visited_mode == 0 || c.opt.visited_mode == vm) trial(T, C, vm, 0);
+    auto choose = [&]() -> const Trial* {
+        long long best_found = 0;
+        for (const Trial& t : trials) best_found = std::max(best_found, t.found);
+        const Trial* pick = nullptr;
+        for (const Trial& t : trials)
+            if ((double)t.found >= (double)best_found * 0.999 && (!pick || t.ms < pick->ms)) pick = &t;
+        return pick;
+    };
+    // stage 2: block size for the chosen shape
+    if (const Trial* p1 = choose(); p1 && c.opt.block_threads == 0) {
+        const Trial t1 = *p1;
+        for (int bt : {32, 64, 128, 256})
+            if (bt != t1.bt) trial(t1.T, t1.C, t1.vm, bt);
+    }
+    release();
+    const Trial* pick = choose();
+    c.T = pick ? pick->T : T0;
+    c.C = pick ? pick->C : C0;
+    c.tuned_vm = pick ? pick->vm : 0;
+    c.tuned_bt = pick ? pick->bt : 0;
+    if (c.cfg.IsDebug) {
+        for (const Trial& t : trials)
+            std::printf("[gmapf] autotune T=%d C=%d visited=%d block=%d: %.3f ms, found %lld/%d\n", t.T, t.C, t.vm,
+                        t.bt, t.ms, t.found, Q);
+        std::printf("[gmapf] autotune picked T=%d C=%d visited=%d block=%d\n", c.T, c.C, c.tuned_vm, c.tuned_bt);
+    }
+    // the sample's searches do not count toward the frames' statistics
+    CK(cudaMemsetAsync(d.stats, 0, sizeof(unsigned long long) * ST_COUNT, d.stream));
+    CK(cudaStreamSynchronize(d.stream));
+    std::memset(c.h_stats, 0, sizeof(unsigned long long) * ST_COUNT);
+    for (int k = 0; k < ST_COUNT; k++) c.stats_prev[k] = 0;
+    return device_reconfigure_search(c, err);
 }
 
 }  // namespace gmapf_b200

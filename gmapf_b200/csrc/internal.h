@@ -256,6 +256,8 @@ struct Context {
     // effective search parameters
     int T = 4, C = 16, block_threads = 128;
     float K = 1.0f;
+    // autotuner's choices where the options leave them open (0: pick by occupancy)
+    int tuned_vm = 0, tuned_bt = 0;
     // device
     Device dev;
     Profiler prof;

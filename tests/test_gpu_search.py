@@ -76,6 +76,33 @@ def test_plain_equals_batched(oracle_mod, vm):
     assert np.array_equal(fb, fp) and np.array_equal(lb, lp) and np.array_equal(pb, pp)
 
 
+def test_autotune_picks_a_shape_and_stays_exact(oracle_mod):
+    scn = S.cfg3(cells=24)
+    g = G.GMAPF()
+    g.Init(G.make_config(4, scn.radius, scn.speed, 4, 8, 32, scn.heuristic_k))
+    g.set_options(autotune=True)
+    S.build_map(g, scn)
+    g.ManualStart()
+    sh = g.search_shape()
+    assert sh["T"] in (2, 4, 8, 16, 32) and sh["C"] in (8, 16, 32, 64, 128, 256)
+    assert sh["visited_mode"] in (1, 2) and sh["block_threads"] in (32, 64, 128, 256)
+    s, t = random_queries(g, scn, 1000, seed=17)
+    check_batch(oracle_mod, g, s, t, sh["T"], sh["C"])
+
+
+def test_autotune_keeps_fixed_options(oracle_mod):
+    scn = S.cfg2()
+    g = G.GMAPF()
+    g.Init(G.make_config(4, scn.radius, scn.speed, 4, 8, 32, scn.heuristic_k))
+    g.set_options(autotune=True, visited_mode=2, block_threads=64)
+    S.build_map(g, scn)
+    g.ManualStart()
+    sh = g.search_shape()
+    assert sh["visited_mode"] == 2 and sh["block_threads"] == 64
+    s, t = random_queries(g, scn, 600, seed=18)
+    check_batch(oracle_mod, g, s, t, sh["T"], sh["C"])
+
+
 def test_longest_first_order_does_not_change_results(oracle_mod):
     scn = S.cfg3(cells=32)
     go = map_world(scn, T=8, Cap=16, order=True)
