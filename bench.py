@@ -46,6 +46,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "p99 step ms & path queries/s at 16k agents, batched vs plain, on 1 B200"
 
 
+VISITED = {1: "shared-memory bitmap", 2: "query-stamped global records", 3: "global bitmap (L2-resident)"}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -370,7 +373,7 @@ def bench_b200(args):
                        "threads_per_agent": Tb, "queue_capacity": Cb, "block_threads": shape["block_threads"],
                        "shape_source": "autotuned per map" if autotune else "Config",
                        "config_threads_per_agent": T, "config_queue_capacity": C,
-                       "visited_mode": "shared-memory bitmap" if shape["visited_mode"] == 1 else "global records",
+                       "visited_mode": VISITED[shape["visited_mode"]],
                        "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",
                        "l2": "flushed between frames (256 MB write); per-frame search records exceed L2",
                        "parallelism": f"{ws} independent scenes (one per GPU)"},

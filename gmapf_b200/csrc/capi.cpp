@@ -149,6 +149,8 @@ gmapf_status gmapf_set_options(gmapf_ctx* ctx, const gmapf_options* o) {
         (o->block_threads < 32 || o->block_threads > 256 || o->block_threads % 32 != 0))
         return fail(GMAPF_E_INVALID_ARG, "block_threads must be 0 or a multiple of 32 in [32, 256]");
     if (o->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
+    if (o->visited_mode < 0 || o->visited_mode > 3)
+        return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
     c.opt = *o;
     if (o->block_threads) c.block_threads = o->block_threads;
     return GMAPF_OK;
@@ -466,7 +468,7 @@ gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t*
     if (T) *T = c.T;
     if (C) *C = c.C;
     if (bt) *bt = c.block_threads;
-    if (vm) *vm = c.dev.smemv ? 1 : 2;
+    if (vm) *vm = c.dev.vm;
     if (slots) *slots = c.dev.slots;
     return GMAPF_OK;
 }

@@ -83,6 +83,7 @@ SearchParams search_params(Context& c) {
     p.rec = d.rec;
     p.epoch = d.epoch;
     p.slots = d.slots;
+    p.gbm = d.gbm;
     p.work_ctr = d.counters + CT_WORK;
     p.max_rounds = 4 * c.map.n + 64;
     p.paths = d.paths;
@@ -162,37 +163,36 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     long long budget = c.opt.search_mem_budget > 0 ? c.opt.search_mem_budget : (40ll << 30);
     budget = std::min<long long>(budget, (long long)(freeb * 0.6));
     const long long per_slot = (long long)std::max(1, c.map.n) * (long long)sizeof(Rec);
-    const long long mem_slots = budget / per_slot;
     d.bm_words = search_bitmap_words(std::max(1, c.map.n));
 
-    // Candidates: visited state on chip (bitmap) or in global records, and
-    // the block size.  The score is the number of resident lane groups, with
-    // on-chip claims counted double (they remove one L2 round trip from every
-    // round).
+    // Candidates: visited placement (1 shared-memory bitmap, 2 stamped
+    // records, 3 global bitmap) and block size.  The score is the number of
+    // resident slots weighted by how close the claim check is: on chip x4,
+    // L2 x3, DRAM x2 (the record check misses L2 in every round).
     long long best_score = -1;
     int best_bt = 0;
-    bool best_smem = false;
+    int best_vm = 2;
     long long best_slots = 0;
     const int want_vm = c.opt.visited_mode ? c.opt.visited_mode : c.tuned_vm;
     const int want_bt = c.opt.block_threads ? c.opt.block_threads : c.tuned_bt;
-    for (int vm = 1; vm <= 2; vm++) {
+    for (int vm = 1; vm <= 3; vm++) {
         if (want_vm != 0 && want_vm != vm) continue;
-        const bool smem = vm == 1;
+        const long long mem_slots = budget / (per_slot + (vm == 3 ? 4ll * d.bm_words : 0));
         const int bts[4] = {128, 64, 32, 256};
         for (int bt : bts) {
             if (want_bt != 0 && bt != want_bt) continue;
             if (bt % c.T) continue;
-            const int per_sm = search_max_blocks_per_sm(c.T, c.C, bt, smem, d.bm_words);
+            const int per_sm = search_max_blocks_per_sm(c.T, c.C, bt, vm, d.bm_words);
             if (per_sm <= 0) continue;
             const int gpb = bt / 32;  // one request slot per warp
             long long slots = std::min((long long)sms * per_sm * gpb, mem_slots);
             slots = (slots / gpb) * gpb;
             if (slots < gpb) continue;
-            const long long score = slots * (smem ? 2 : 1);
+            const long long score = slots * (vm == 1 ? 4 : vm == 3 ? 3 : 2);
             if (score > best_score) {
                 best_score = score;
                 best_bt = bt;
-                best_smem = smem;
+                best_vm = vm;
                 best_slots = slots;
             }
         }
@@ -203,11 +203,11 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
         return GMAPF_E_CAPACITY;
     }
     c.block_threads = best_bt;
-    d.smemv = best_smem;
+    d.vm = best_vm;
     d.slots = (int)best_slots;
     blocks = (int)(best_slots / (best_bt / 32));
     // leave the kernel's shared-memory limit set for the chosen shape
-    search_max_blocks_per_sm(c.T, c.C, best_bt, best_smem, d.bm_words);
+    search_max_blocks_per_sm(c.T, c.C, best_bt, best_vm, d.bm_words);
     return GMAPF_OK;
 }
 
@@ -218,13 +218,14 @@ int alloc_search_state(Context& c, std::string& err) {
     if (rc) return rc;
     DALLOC(d.rec, (size_t)d.slots * std::max(1, c.map.n));
     DALLOC(d.epoch, (size_t)d.slots);
+    if (d.vm == 3) DALLOC(d.gbm, (size_t)d.slots * d.bm_words);
     return GMAPF_OK;
 }
 
 void free_search_state(Context& c) {
     Device& d = c.dev;
     for (void*& p : d.allocs) {
-        if (p == (void*)d.rec || p == (void*)d.epoch) {
+        if (p == (void*)d.rec || p == (void*)d.epoch || (p && p == (void*)d.gbm)) {
             cudaFree(p);
             p = nullptr;
         }
@@ -232,6 +233,7 @@ void free_search_state(Context& c) {
     d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), nullptr), d.allocs.end());
     d.rec = nullptr;
     d.epoch = nullptr;
+    d.gbm = nullptr;
     d.slots = 0;
 }
 
@@ -261,7 +263,7 @@ int enqueue_frame(Context& c, bool timing, std::string& err) {
         launch_order_requests(s, d.req, d.counters + CT_REQ, d.req_sorted, d.req_keys, d.lm, d.lm_count, c.map.n);
         sp.req = d.req_sorted;
     }
-    CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.smemv, d.bm_words));
+    CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.vm, d.bm_words));
     if (timing) CK(cudaEventRecordWithFlags(d.ev[2], s, cudaEventRecordExternal));
     // mover branch
     MoverParams mp = mover_params(c);
@@ -486,7 +488,7 @@ int device_async_step(Context& c, float dt, std::string& err) {
                 const int cnt = std::min(chunk, R - base);
                 const int gpb = c.block_threads / 32;
                 const int blocks = (cnt + gpb - 1) / gpb;
-                CK(launch_search(s, sp, blocks, c.block_threads, false, base, d.smemv, d.bm_words));
+                CK(launch_search(s, sp, blocks, c.block_threads, false, base, d.vm, d.bm_words));
                 c.launches += 1;
             }
         }
@@ -645,14 +647,14 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
     CK(cudaEventRecord(d.ev[6], s));
     if (n > 0) {
         if (c.opt.mode == GMAPF_MODE_BATCHED) {
-            CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.smemv, d.bm_words));
+            CK(launch_search(s, sp, search_blocks(c), c.block_threads, true, 0, d.vm, d.bm_words));
             c.launches += 1;
         } else {
             sp.req_count_h = n;
             const int gpb = c.block_threads / 32;
             for (int base = 0; base < n; base += d.slots) {
                 const int cnt = std::min(d.slots, n - base);
-                CK(launch_search(s, sp, (cnt + gpb - 1) / gpb, c.block_threads, false, base, d.smemv, d.bm_words));
+                CK(launch_search(s, sp, (cnt + gpb - 1) / gpb, c.block_threads, false, base, d.vm, d.bm_words));
                 c.launches += 1;
             }
         }
@@ -818,7 +820,7 @@ int device_autotune(Context& c, std::string& err) {
             if (ms > 3.0f * best_so_far) break;
         }
         best_so_far = std::min(best_so_far, ms);
-        trials.push_back({T, C, c.dev.smemv ? 1 : 2, c.block_threads, ms, (long long)st.found});
+        trials.push_back({T, C, c.dev.vm, c.block_threads, ms, (long long)st.found});
     };
     // stage 1: threads per agent x queue capacity x visited placement, block
     // size by occupancy
@@ -826,7 +828,7 @@ int device_autotune(Context& c, std::string& err) {
     if (std::find(Cs.begin(), Cs.end(), C0) == Cs.end()) Cs.push_back(C0);
     for (int T : Ts)
         for (int C : Cs)
-            for (int vm = 1; vm <= 2; vm++)
+            for (int vm = 1; vm <= 3; vm++)
                 if (c.opt.visited_mode == 0 || c.opt.visited_mode == vm) trial(T, C, vm, 0);
     auto choose = [&]() -> const Trial* {
         long long best_found = 0;

@@ -58,6 +58,7 @@ struct SearchParams {
     Rec* rec;                // slots * n
     unsigned* epoch;         // per slot
     int slots;
+    unsigned* gbm;           // visited mode 3: bm_words 32-bit words per slot, global
     int* work_ctr;
     int max_rounds;
     // outputs
@@ -128,13 +129,14 @@ void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets,
 // search.cu
 // persistent: groups pull requests from *work_ctr until *req_count_d is reached.
 // plain: one request per group, requests [base, base + groups).
-// smem_visited: visited bitmap in shared memory (bm_words 32-bit words per
-// lane group) instead of stamped records in global memory.
+// vm (visited state): 1 a 2-bit bitmap per slot in shared memory (bm_words
+// 32-bit words per slot), 2 query-stamped records in global memory, 3 a 2-bit
+// bitmap per slot in global memory (p.gbm, small enough to stay in L2).
 cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int block_threads,
-                          bool persistent, int req_base, bool smem_visited, int bm_words);
+                          bool persistent, int req_base, int vm, int bm_words);
 size_t search_smem_bytes(int C, int block_threads, int bm_words_per_group, int T);
 int search_bitmap_words(int n_nodes);
-int search_max_blocks_per_sm(int T, int C, int block_threads, bool smem_visited, int bm_words);
+int search_max_blocks_per_sm(int T, int C, int block_threads, int vm, int bm_words);
 
 // ------------------------------------------------------------------- host --
 
@@ -196,8 +198,9 @@ struct Device {
     Rec* rec = nullptr;
     unsigned* epoch = nullptr;
     int slots = 0;
-    bool smemv = false;  // visited bitmap in shared memory
-    int bm_words = 0;    // bitmap words per lane group
+    int vm = 2;                 // visited mode (1, 2 or 3; see launch_search)
+    unsigned* gbm = nullptr;    // visited mode 3: slots x bm_words
+    int bm_words = 0;           // bitmap words per slot
     // agent grid
     int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
         *cell_items = nullptr;

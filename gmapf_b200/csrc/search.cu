@@ -31,9 +31,11 @@
 //     T = 32), so thread order is candidate order and a single
 //     __match_any_sync per pass resolves every claim of the pass: the lowest
 //     fresh thread of a node claims it, later ones see the claim;
-//   - visited state: a 2-bit-per-node bitmap (claimed, side) in shared memory
-//     when it fits, else a 32-byte record per (slot, node) in global memory
-//     stamped with the query epoch (no clearing between queries);
+//   - visited state, one of three placements: a 2-bit-per-node bitmap
+//     (claimed, side) per slot in shared memory; the same bitmap per slot in
+//     global memory, sized to stay in L2 and cleared per query; or the
+//     32-byte records themselves, stamped with the query epoch (no clearing
+//     between queries, but one DRAM round trip per round);
 //   - records (G, parent and five further ancestors) are written once per
 //     claimed node; the path walk reads one record per six hops; a node's
 //     record is read when it is expanded, in flight together with its row;
@@ -117,9 +119,8 @@ __device__ __forceinline__ void st_rec(Rec* r, unsigned stamp, int gd, int a0, i
 }
 
 // 2-bit visited state: bit 0 = claimed, bit 1 = reached from the start
-__device__ __forceinline__ int bm_get(const unsigned* bm, int n) {
-    return (int)((bm[n >> 4] >> ((n & 15) << 1)) & 3u);
-}
+__device__ __forceinline__ int bm_bits(unsigned w, int n) { return (int)((w >> ((n & 15) << 1)) & 3u); }
+__device__ __forceinline__ int bm_get(const unsigned* bm, int n) { return bm_bits(bm[n >> 4], n); }
 __device__ __forceinline__ void bm_set(unsigned* bm, int n, int dir) {
     atomicOr(bm + (n >> 4), (1u | ((unsigned)dir << 1)) << ((n & 15) << 1));
 }
@@ -135,8 +136,13 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
 }
 
 
-template <int T, bool SMEMV>
+// VM: visited placement (1 shared-memory bitmap, 2 stamped records, 3 global
+// bitmap).  In modes 1 and 3 a bit set by one thread is seen by the others
+// after the next __syncwarp (bar.warp.sync orders memory among its threads).
+template <int T, int VM>
 __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
+    constexpr bool SMEMV = VM == 1;  // bitmap in shared memory
+    constexpr bool BMV = VM != 2;    // visited state in a bitmap (shared or global)
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;                 // warp in block
@@ -156,9 +162,11 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
     ring.q = lane < T ? lane : 0;
     ring.C = C;
     int* fr = base + (size_t)wpb * qblk + (size_t)wib * fblk;  // word w of item i at fr[w*3T + i]
-    unsigned* bm = reinterpret_cast<unsigned*>(base + (size_t)wpb * (qblk + fblk)) + (size_t)wib * bm_words;
+    unsigned* bm = SMEMV ? reinterpret_cast<unsigned*>(base + (size_t)wpb * (qblk + fblk)) + (size_t)wib * bm_words
+                         : nullptr;
 
     if (slot >= p.slots) return;  // whole warps
+    if (VM == 3) bm = p.gbm + (size_t)slot * bm_words;
     Rec* rec = p.rec + (size_t)slot * n_nodes;
     const unsigned lt_mask = (1u << lane) - 1u;
 
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         }
 
         unsigned ep = 0;
-        if (!SMEMV) {
+        if (VM == 2) {
             unsigned e = 0;
             if (lane == 0) e = p.epoch[slot] + 1u;
             e = __shfl_sync(kFull, e, 0);
@@ -205,9 +213,12 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
             }
             if (lane == 0) p.epoch[slot] = e;
             ep = e;
-        } else {
+        } else if (SMEMV) {
             uint4* b4 = reinterpret_cast<uint4*>(bm);
             for (int k = lane; k < (bm_words >> 2); k += 32) b4[k] = make_uint4(0, 0, 0, 0);
+        } else {
+            uint4* b4 = reinterpret_cast<uint4*>(bm);
+            for (int k = lane; k < (bm_words >> 2); k += 32) __stcg(b4 + k, make_uint4(0, 0, 0, 0));
         }
         __syncwarp();
         const float2 cs = p.cen[start];
@@ -234,7 +245,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
             uid = node;
             ugd = gd;
             st_rec(rec + node, ep, gd, -1, -1, -1, -1, -1, -1);
-            if (SMEMV) bm_set(bm, node, gd);
+            if (BMV) bm_set(bm, node, gd);
         }
         (void)f0;  // the seeds' F never takes part in a comparison: each seed is alone in its queue
         __syncwarp();
@@ -263,8 +274,11 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 bool prev = false;
                 int pgd = 0, pknown = 0;
                 if (valid) {
-                    if (SMEMV) {
-                        const int st = bm_get(bm, n);  // includes earlier passes of this round
+                    if (BMV) {
+                        // mode 1: includes earlier passes of this round; mode 3:
+                        // the word loaded for this pass (after the previous
+                        // pass's __syncwarp)
+                        const int st = SMEMV ? bm_get(bm, n) : bm_bits((unsigned)cst.x, n);
                         prev = (st & 1) != 0;
                         pgd = st >> 1;                 // side only; G read at the meet
                     } else {
@@ -294,7 +308,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 } else if (prev) {
                     cgd = pgd;
                     cknown = pknown;
-                    conflict = (SMEMV ? pgd : (pgd & 1)) != du;
+                    conflict = (BMV ? pgd : (pgd & 1)) != du;
                 }
                 const unsigned cm = __ballot_sync(kFull, conflict);
                 if (!meet && cm != 0u) {  // warp-uniform
@@ -316,7 +330,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                     fr[idx] = __float_as_int(F);
                     fr[3 * T + idx] = ngd;
                     fr[6 * T + idx] = n;
-                    if (SMEMV) bm_set(bm, n, du);
+                    if (BMV) bm_set(bm, n, du);
                     // ancestors 1..5 of n = ancestors 0..4 of the popped node
                     st_rec(rec + n, ep, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
                 }
@@ -364,7 +378,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                         expansions++;
                         deg_sum += (unsigned)r0.w;
                     }
-                    if (!SMEMV && valid) cst = ld_state(rec + n);  // claims of earlier rounds
+                    if (VM == 2 && valid) cst = ld_state(rec + n);  // claims of earlier rounds
+                    if (VM == 3 && valid) cst.x = (int)__ldcg(bm + (n >> 4));
                 }
                 deferred_queue_work();
                 resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, false);
@@ -405,7 +420,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                         ld_rec(rec + cu, ra, rb);
                         cx = cc.x;
                         cy = cc.y;
-                        if (!SMEMV) cst = ld_state(rec + n);
+                        if (VM == 2) cst = ld_state(rec + n);
+                        if (VM == 3) cst.x = (int)__ldcg(bm + (n >> 4));
                     }
                     resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, base > 0);
                 }
@@ -534,55 +550,55 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
     }
 }
 
-template <int T, bool SMEMV>
+template <int T, int VM>
 cudaError_t launch_t(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
                      int req_base, int bm_words) {
     // the dynamic shared-memory limit was raised when the search state was
     // sized (no attribute calls here: this may run under stream capture)
-    const size_t smem = search_smem_bytes(p.C, bt, SMEMV ? bm_words : 0, T);
+    const size_t smem = search_smem_bytes(p.C, bt, VM == 1 ? bm_words : 0, T);
     if (blocks <= 0) return cudaSuccess;
-    k_search<T, SMEMV><<<blocks, bt, smem, s>>>(p, persistent ? 1 : 0, req_base, bm_words);
+    k_search<T, VM><<<blocks, bt, smem, s>>>(p, persistent ? 1 : 0, req_base, bm_words);
     return cudaGetLastError();
 }
 
-template <int T, bool SMEMV>
+template <int T, int VM>
 int occupancy_t(int C, int bt, int bm_words) {
-    const size_t smem = search_smem_bytes(C, bt, SMEMV ? bm_words : 0, T);
+    const size_t smem = search_smem_bytes(C, bt, VM == 1 ? bm_words : 0, T);
     if (smem > 227 * 1024) return 0;
-    if (cudaFuncSetAttribute(k_search<T, SMEMV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    if (cudaFuncSetAttribute(k_search<T, VM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<T, SMEMV>, bt, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<T, VM>, bt, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     return nb;
 }
 
-template <bool SMEMV>
+template <int VM>
 cudaError_t launch_v(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
                      int req_base, int bm_words) {
     switch (p.T) {
-        case 2: return launch_t<2, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
-        case 4: return launch_t<4, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
-        case 8: return launch_t<8, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
-        case 16: return launch_t<16, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
-        case 32: return launch_t<32, SMEMV>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 2: return launch_t<2, VM>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 4: return launch_t<4, VM>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 8: return launch_t<8, VM>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 16: return launch_t<16, VM>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 32: return launch_t<32, VM>(s, p, blocks, bt, persistent, req_base, bm_words);
         default: return cudaErrorInvalidValue;
     }
 }
 
-template <bool SMEMV>
+template <int VM>
 int occupancy_v(int T, int C, int bt, int bm_words) {
     switch (T) {
-        case 2: return occupancy_t<2, SMEMV>(C, bt, bm_words);
-        case 4: return occupancy_t<4, SMEMV>(C, bt, bm_words);
-        case 8: return occupancy_t<8, SMEMV>(C, bt, bm_words);
-        case 16: return occupancy_t<16, SMEMV>(C, bt, bm_words);
-        case 32: return occupancy_t<32, SMEMV>(C, bt, bm_words);
+        case 2: return occupancy_t<2, VM>(C, bt, bm_words);
+        case 4: return occupancy_t<4, VM>(C, bt, bm_words);
+        case 8: return occupancy_t<8, VM>(C, bt, bm_words);
+        case 16: return occupancy_t<16, VM>(C, bt, bm_words);
+        case 32: return occupancy_t<32, VM>(C, bt, bm_words);
         default: return 0;
     }
 }
@@ -590,7 +606,7 @@ int occupancy_v(int T, int C, int bt, int bm_words) {
 }  // namespace
 
 // per-block dynamic shared memory, per warp: T queues of C entries (12 B),
-// a frontier of 3T entries (12 B) and, on-chip mode, the visited bitmap
+// a frontier of 3T entries (12 B) and, in visited mode 1, the visited bitmap
 size_t search_smem_bytes(int C, int bt, int bm_words_per_warp, int T) {
     const size_t warps = (size_t)bt / 32;
     return warps * 4 * (search_queue_words(C, T) + search_frontier_words(T) + (size_t)bm_words_per_warp);
@@ -601,14 +617,23 @@ int search_bitmap_words(int n_nodes) {
     return (w + 3) & ~3;  // whole uint4 for the clear
 }
 
-int search_max_blocks_per_sm(int T, int C, int bt, bool smem_visited, int bm_words) {
-    return smem_visited ? occupancy_v<true>(T, C, bt, bm_words) : occupancy_v<false>(T, C, bt, 0);
+int search_max_blocks_per_sm(int T, int C, int bt, int vm, int bm_words) {
+    switch (vm) {
+        case 1: return occupancy_v<1>(T, C, bt, bm_words);
+        case 2: return occupancy_v<2>(T, C, bt, 0);
+        case 3: return occupancy_v<3>(T, C, bt, 0);
+        default: return 0;
+    }
 }
 
 cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int bt, bool persistent,
-                          int req_base, bool smem_visited, int bm_words) {
-    return smem_visited ? launch_v<true>(s, p, blocks, bt, persistent, req_base, bm_words)
-                        : launch_v<false>(s, p, blocks, bt, persistent, req_base, 0);
+                          int req_base, int vm, int bm_words) {
+    switch (vm) {
+        case 1: return launch_v<1>(s, p, blocks, bt, persistent, req_base, bm_words);
+        case 2: return launch_v<2>(s, p, blocks, bt, persistent, req_base, 0);
+        case 3: return launch_v<3>(s, p, blocks, bt, persistent, req_base, bm_words);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace gmapf_b200

@@ -88,7 +88,8 @@ typedef struct gmapf_options {
     int64_t search_mem_budget; /* bytes for per-slot search records, 0 = automatic */
     int32_t order_by_estimate; /* 1 (default): batched form serves the searches with the largest
                                   landmark hop-distance estimate first; results do not depend on it */
-    int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records */
+    int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records,
+                                  3 global bitmap per slot (L2-resident for maps up to a few 100k triangles) */
     int32_t _reserved[4];
 } gmapf_options;
 

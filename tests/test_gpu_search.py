@@ -28,7 +28,7 @@ def check_batch(oracle_mod, g, starts, targets, T, Cap, K=1.0):
     return f, l, p, st
 
 
-@pytest.mark.parametrize("vm", [1, 2])
+@pytest.mark.parametrize("vm", [1, 2, 3])
 @pytest.mark.parametrize("T,Cap", [(2, 1), (2, 16), (4, 16), (8, 2), (32, 64)])
 def test_cfg1_all_pairs(oracle_mod, T, Cap, vm):
     scn = S.cfg1()
@@ -39,7 +39,7 @@ def test_cfg1_all_pairs(oracle_mod, T, Cap, vm):
     assert f.mean() > 0.5
 
 
-@pytest.mark.parametrize("vm", [1, 2])
+@pytest.mark.parametrize("vm", [1, 2, 3])
 @pytest.mark.parametrize("T,Cap", [(8, 32), (4, 16), (16, 8)])
 def test_cfg2_random(oracle_mod, T, Cap, vm):
     scn = S.cfg2()
@@ -48,8 +48,8 @@ def test_cfg2_random(oracle_mod, T, Cap, vm):
     check_batch(oracle_mod, g, s, t, T, Cap)
 
 
-@pytest.mark.parametrize("vm", [1, 2])
-@pytest.mark.parametrize("T,Cap", [(8, 32), (32, 64), (2, 256)])
+@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("T,Cap", [(8, 32), (32, 64), (2, 256), (16, 16)])
 def test_maze64_random(oracle_mod, T, Cap, vm):
     scn = S.cfg3(cells=64)
     g = map_world(scn, T=T, Cap=Cap, visited_mode=vm)
@@ -65,11 +65,11 @@ def test_maze64_random(oracle_mod, T, Cap, vm):
                 assert b in nb[a]
 
 
-@pytest.mark.parametrize("vm", [1, 2])
+@pytest.mark.parametrize("vm", [1, 2, 3])
 def test_plain_equals_batched(oracle_mod, vm):
     scn = S.cfg2()
     gb = map_world(scn, T=8, Cap=32, mode=G.MODE_BATCHED, visited_mode=vm)
-    gp = map_world(scn, T=8, Cap=32, mode=G.MODE_PLAIN, visited_mode=3 - vm)
+    gp = map_world(scn, T=8, Cap=32, mode=G.MODE_PLAIN, visited_mode=vm % 3 + 1)
     s, t = random_queries(gb, scn, 1500, seed=13)
     fb, lb, pb, _ = gb.search_batch(s, t, gb.node_count)
     fp, lp, pp, _ = gp.search_batch(s, t, gp.node_count)
@@ -85,7 +85,7 @@ def test_autotune_picks_a_shape_and_stays_exact(oracle_mod):
     g.ManualStart()
     sh = g.search_shape()
     assert sh["T"] in (2, 4, 8, 16, 32) and sh["C"] in (8, 16, 32, 64, 128, 256)
-    assert sh["visited_mode"] in (1, 2) and sh["block_threads"] in (32, 64, 128, 256)
+    assert sh["visited_mode"] in (1, 2, 3) and sh["block_threads"] in (32, 64, 128, 256)
     s, t = random_queries(g, scn, 1000, seed=17)
     check_batch(oracle_mod, g, s, t, sh["T"], sh["C"])
 
@@ -122,9 +122,10 @@ def test_block_shape_does_not_change_results(oracle_mod, bt):
     check_batch(oracle_mod, g, s, t, 4, 16)
 
 
-def test_edge_cases(oracle_mod):
+@pytest.mark.parametrize("vm", [1, 2, 3])
+def test_edge_cases(oracle_mod, vm):
     scn = S.cfg1()
-    g = map_world(scn, T=4, Cap=16)
+    g = map_world(scn, T=4, Cap=16, visited_mode=vm)
     n = g.node_count
     # empty batch
     f, l, p, st = g.search_batch(np.zeros(0, np.int32), np.zeros(0, np.int32), n)
@@ -144,10 +145,12 @@ def test_edge_cases(oracle_mod):
     assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
 
 
-def test_disconnected_map_not_found(oracle_mod):
+@pytest.mark.parametrize("vm", [1, 2, 3])
+def test_disconnected_map_not_found(oracle_mod, vm):
     # two separate triangles: searches between them exhaust both queues
     g = G.GMAPF()
     g.Init(G.make_config(4, 1, 1, 4, 4, 16))
+    g.set_options(visited_mode=vm)
     nodes = np.zeros(4, G.NODE_DTYPE)
     nodes["P1"] = [[0, 0], [1, 0], [10, 0], [11, 0]]
     nodes["P2"] = [[1, 0], [1, 1], [11, 0], [11, 1]]

@@ -68,7 +68,7 @@ def test_cfg1_200_steps(oracle_mod):
     assert np.array_equal(pos, d["pos"], equal_nan=True)
 
 
-@pytest.mark.parametrize("vm", [1, 2])
+@pytest.mark.parametrize("vm", [1, 2, 3])
 def test_cfg2_retargets(oracle_mod, vm):
     scn = S.cfg2()
     g, ow, rng = make_pair(oracle_mod, scn, 512, vm=vm)
