@@ -191,7 +191,9 @@ def make_scene(cells, seed, T, C, mode, agents, profiler=True, autotune=False):
     from gmapf_b200 import scenarios as S
     scn = S.cfg3(cells=cells, seed=seed, agents=agents, threads_per_agent=T, queue_capacity=C)
     g, starts, rng = S.make_world(scn, mode=mode, profiler=profiler, autotune=autotune)
-    g.ManualStart()
+    t0 = time.perf_counter()
+    g.ManualStart()  # device upload, landmarks and (batched) the autotuner
+    g.startup_s = time.perf_counter() - t0
     return scn, g, rng
 
 
@@ -372,6 +374,7 @@ def bench_b200(args):
                                    f"retargeted every frame", "triangles": n_nodes, "agents": A,
                        "threads_per_agent": Tb, "queue_capacity": Cb, "block_threads": shape["block_threads"],
                        "shape_source": "autotuned per map" if autotune else "Config",
+                       "start_s": round(g.startup_s, 2),
                        "config_threads_per_agent": T, "config_queue_capacity": C,
                        "visited_mode": VISITED[shape["visited_mode"]],
                        "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",

@@ -757,13 +757,14 @@ int device_autotune(Context& c, std::string& err) {
     Device& d = c.dev;
     const int n = c.map.n;
     if (n < 2) return GMAPF_OK;
-    // the sample is as large as a frame's request batch (2,048..8,192), so that
-    // the tuner weighs throughput as a frame does, with its path rows kept
-    // under 8 GB and a quarter of the free memory
+    // the sample is as large as a frame's request batch (2,048..16,384), so
+    // that the tuner weighs throughput against the longest searches as a
+    // frame does, with its path rows kept under 8 GB and a quarter of the free
+    // memory
     size_t freeb = 0, totalb = 0;
     CK(cudaMemGetInfo(&freeb, &totalb));
     const double row_cap = std::min(8e9, 0.25 * (double)freeb);
-    int Q = std::min(8192, std::max(2048, c.cfg.PathFinderParallelAgents));
+    int Q = std::min(16384, std::max(2048, c.cfg.PathFinderParallelAgents));
     while (Q > 128 && (double)Q * n * 4 > row_cap) Q /= 2;
     std::vector<int> hs(Q), ht(Q);
     unsigned long long x = 0x9e3779b97f4a7c15ull;
@@ -823,13 +824,22 @@ int device_autotune(Context& c, std::string& err) {
         trials.push_back({T, C, c.dev.vm, c.block_threads, ms, (long long)st.found});
     };
     // stage 1: threads per agent x queue capacity x visited placement, block
-    // size by occupancy
+    // size by occupancy.  The found count depends on (T, C) only, so a shape
+    // already below the best found count skips its other placements.
     std::vector<int> Ts = {32, 16, 8, 4, 2}, Cs = {8, 16, 32, 64, 128, 256};  // likely-fast shapes first
     if (std::find(Cs.begin(), Cs.end(), C0) == Cs.end()) Cs.push_back(C0);
+    long long best_found_so_far = 0;
     for (int T : Ts)
         for (int C : Cs)
-            for (int vm = 1; vm <= 3; vm++)
-                if (c.opt.visited_mode == 0 || c.opt.visited_mode == vm) trial(T, C, vm, 0);
+            for (int vm : {3, 2, 1}) {
+                if (c.opt.visited_mode != 0 && c.opt.visited_mode != vm) continue;
+                const size_t before = trials.size();
+                trial(T, C, vm, 0);
+                if (trials.size() == before) continue;  // shape does not fit this placement
+                const long long f = trials.back().found;
+                best_found_so_far = std::max(best_found_so_far, f);
+                if ((double)f < (double)best_found_so_far * 0.999) break;
+            }
     auto choose = [&]() -> const Trial* {
         long long best_found = 0;
         for (const Trial& t : trials) best_found = std::max(best_found, t.found);

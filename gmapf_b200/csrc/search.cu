@@ -131,8 +131,10 @@ constexpr unsigned kFull = 0xffffffffu;
 __host__ __device__ __forceinline__ size_t search_queue_words(int C, int T) {
     return ((size_t)kEntryWords * C * T + 3) & ~(size_t)3;
 }
+// the round's frontier (3T entries of 3 words) and, for T >= 16, the owner
+// lane of each of the 3T compacted candidates
 __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
-    return ((size_t)kEntryWords * 3 * T + 3) & ~(size_t)3;
+    return ((size_t)kEntryWords * 3 * T + (T >= 16 ? 3 * (size_t)T : 0) + 3) & ~(size_t)3;
 }
 
 
@@ -272,46 +274,45 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                 const int du = cgdu & 1;
                 const int ngd = (((cgdu >> 1) + 1) << 1) | du;
                 bool prev = false;
-                int pgd = 0, pknown = 0;
+                int pside = 0, pgd = 0, pknown = 0;  // earlier claim: side, G<<1|side if known
                 if (valid) {
-                    if (BMV) {
-                        // mode 1: includes earlier passes of this round; mode 3:
-                        // the word loaded for this pass (after the previous
-                        // pass's __syncwarp)
-                        const int st = SMEMV ? bm_get(bm, n) : bm_bits((unsigned)cst.x, n);
+                    if (VM == 1) {  // includes earlier passes of this round
+                        const int st = bm_get(bm, n);
                         prev = (st & 1) != 0;
-                        pgd = st >> 1;                 // side only; G read at the meet
+                        pside = st >> 1;
+                    } else if (VM == 3) {  // word loaded at the start of the round
+                        const int st = bm_bits((unsigned)cst.x, n);
+                        prev = (st & 1) != 0;
+                        pside = st >> 1;
                     } else {
                         prev = (unsigned)cst.x == ep;
                         pgd = cst.y;
+                        pside = pgd & 1;
                         pknown = 1;
-                        if (later_pass && !prev) {  // claimed by an earlier pass of this round
-                            int hit = -1;
-                            for (int w = 0; w < nwin; w++) hit = (fr[6 * T + w] == n) ? w : hit;
-                            if (hit >= 0) {
-                                prev = true;
-                                pgd = fr[3 * T + hit];
-                            }
+                    }
+                    if (VM == 2 && later_pass && !prev) {  // claimed by an earlier pass of this round
+                        int hit = -1;
+                        for (int w = 0; w < nwin; w++) hit = (fr[6 * T + w] == n) ? w : hit;
+                        if (hit >= 0) {
+                            prev = true;
+                            pgd = fr[3 * T + hit];
+                            pside = pgd & 1;
+                            pknown = 1;
                         }
                     }
                 }
                 const bool fresh = valid && !prev;
-                const unsigned mm = __match_any_sync(kFull, fresh ? n : (-1 - lane));
+                const unsigned dm = __ballot_sync(kFull, du);  // candidates' sides
+                const unsigned mm = __match_any_sync(kFull, fresh ? n : -1);
                 const int leader = __ffs(mm) - 1;
                 const bool win = fresh && leader == lane;
-                const int lgd = __shfl_sync(kFull, ngd, leader);
-                bool conflict = false;
-                int cgd = 0, cknown = 1;
-                if (fresh && !win) {
-                    cgd = lgd;
-                    conflict = (lgd & 1) != du;
-                } else if (prev) {
-                    cgd = pgd;
-                    cknown = pknown;
-                    conflict = (BMV ? pgd : (pgd & 1)) != du;
-                }
+                const bool dup = fresh && !win;  // same node as a lower candidate of this pass
+                const bool conflict = dup ? (int)((dm >> leader) & 1u) != du : (prev && pside != du);
                 const unsigned cm = __ballot_sync(kFull, conflict);
                 if (!meet && cm != 0u) {  // warp-uniform
+                    const int lgd = __shfl_sync(kFull, ngd, leader);
+                    const int cgd = dup ? lgd : pgd;
+                    const int cknown = dup ? 1 : pknown;
                     const int ml = __ffs(cm) - 1;
                     mu = __shfl_sync(kFull, cu, ml);
                     mgu = __shfl_sync(kFull, cgdu, ml);
@@ -397,13 +398,19 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                     deg_sum += (unsigned)r0.w;
                 }
                 const int n0 = __popc(b0), n1 = __popc(b1), total = n0 + n1 + __popc(b2);
+                // each owner writes its lane at its candidates' compacted positions
+                // (a ballot rank is one popc; the inverse, the n-th set bit, is not)
+                int* oix = fr + 9 * T;
+                if (idu >= 0) {
+                    if (r0.w > 0) oix[__popc(b0 & lt_mask)] = lane;
+                    if (r0.w > 1) oix[n0 + __popc(b1 & lt_mask)] = lane;
+                    if (r0.w > 2) oix[n0 + n1 + __popc(b2 & lt_mask)] = lane;
+                }
+                __syncwarp();
                 for (int base = 0; base < total; base += 32) {  // warp-uniform
                     const int t = base + lane;
                     const int sl = t < n0 ? 0 : (t < n0 + n1 ? 1 : 2);
-                    const unsigned bm_s = sl == 0 ? b0 : (sl == 1 ? b1 : b2);
-                    const int rank = t - (sl == 0 ? 0 : (sl == 1 ? n0 : n0 + n1));
-                    // the lane holding the (rank+1)-th set bit of this slot's ballot
-                    const int qq = t < total ? (int)(__fns(bm_s, 0, rank + 1) & 31u) : 0;
+                    const int qq = t < total ? (oix[t] & 31) : 0;  // the candidate's owner lane
                     const int cu = __shfl_sync(kFull, idu, qq);
                     const int cgdu = __shfl_sync(kFull, gdu, qq);
                     const int na = __shfl_sync(kFull, r0.x, qq);
