@@ -164,14 +164,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def measured_traffic(cells: int, T: int, C: int, queries_per_step: float):
+def measured_traffic(cells: int, T: int, C: int, vm: int, queries_per_step: float):
     """DRAM bytes per search launch from the committed ncu capture
     (profiles/search_traffic.json, per query, scaled to this frame's
-    queries), or None when no capture matches this workload."""
+    queries), or None when no capture matches this workload and shape."""
     p = ROOT / "profiles" / "search_traffic.json"
     if not p.exists():
         return None, None
-    d = json.loads(p.read_text()).get(f"maze{cells}_T{T}_C{C}")
+    d = json.loads(p.read_text()).get(f"maze{cells}_T{T}_C{C}_vm{vm}")
     if not d:
         return None, None
     return d["bytes_per_query"] * queries_per_step, d["source"]
@@ -312,7 +312,7 @@ def bench_b200(args):
     ab = [algorithmic_bytes(s, n_nodes) for s in dstats]
     achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic, traffic_src = measured_traffic(args.cells, Tb, Cb, queries / max(1, K))
+    traffic, traffic_src = measured_traffic(args.cells, Tb, Cb, shape["visited_mode"], queries / max(1, K))
 
     # batched form at the Config's own shape (same arithmetic as the plain form)
     fixed = None
