@@ -250,6 +250,20 @@ def run_frames_host(g, sets, warmup, steps):
     return wall, stats
 
 
+def path_quality(g, sample):
+    """Hop count over the BFS optimum and centroid polyline length over the
+    FP64 Dijkstra optimum, for a sample of the last frame's agents (their
+    start is the current triangle: nobody moves in a full-retarget frame)."""
+    from gmapf_b200 import path_quality as PQ
+    d = g.debug_agents()
+    ids = np.random.default_rng(5).choice(len(d["cur_node"]), size=min(sample, len(d["cur_node"])), replace=False)
+    ids.sort()
+    paths = [g.path(int(i)) for i in ids]
+    q = PQ.summary(g.map_nodes(), d["cur_node"][ids], d["targ_node"][ids], d["path_len"][ids], paths)
+    q["sample"] = f"{len(ids)} agents of the last timed frame (found paths with start != target)"
+    return q
+
+
 def pct(v, q):
     return float(np.percentile(np.asarray(v, np.float64), q, method="higher")) if len(v) else None
 
@@ -296,6 +310,11 @@ def bench_b200(args):
     queries = float(sum(s["requests"] for s in dstats))
     all_queries = reduce_sum(dist, queries)
     value = all_queries / (dev_total_ms / 1e3)
+
+    # path quality of the last device-timed frame (sample; outside the timing)
+    quality = None
+    if rank == 0 and args.quality_sample > 0:
+        quality = path_quality(g, args.quality_sample)
 
     # e2e through the host API (fresh targets, same scene)
     sets_e2e = target_sets(g, scn, rng, W + K, A)
@@ -387,6 +406,7 @@ def bench_b200(args):
             "expansions_per_s": st_sum["expansions"] / (sum(ms) / 1e3),
             "plain": plain,
             "batched_config_shape": fixed,
+            "path_quality": quality,
             "batched_over_plain": (e2e_value / plain["value"]) if plain else None,
             "roofline": {"bound": "hbm", "kernel": "k_search", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
@@ -466,6 +486,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=2048)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--quality-sample", type=int, default=128, help="agents whose paths are compared with BFS/Dijkstra")
     ap.add_argument("--no-autotune", action="store_true", help="batched form at the Config's T and C")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
