@@ -285,7 +285,7 @@ gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_id
     if (n < 0 || (n > 0 && (!d_ids || !d_pos))) return fail(GMAPF_E_INVALID_ARG, "bad device arrays");
     if (n == 0) return GMAPF_OK;
     std::string err;
-    int rc = device_set_targets_device(c, d_ids, d_pos, n, err);
+    int rc = device_set_targets_device(c, d_ids, d_pos, n, 0, c.A, err);
     if (rc) return fail(rc, err);
     return GMAPF_OK;
 }

@@ -96,6 +96,64 @@ SearchParams search_params(Context& c) {
     return p;
 }
 
+// The scene table of a plain context: its one map and all its agents.
+SceneInfo single_scene(const Context& c) {
+    const HostMap& m = c.map;
+    SceneInfo si;
+    si.node_base = 0;
+    si.n = m.n;
+    si.agent_base = 0;
+    si.A = c.A;
+    si.P = c.cfg.PathFinderParallelAgents;
+    si.radius = c.cfg.AgentRadius;
+    si.speed = c.cfg.AgentSpeed;
+    si.bx0 = m.bx0;
+    si.by0 = m.by0;
+    si.bx1 = m.bx1;
+    si.by1 = m.by1;
+    si.gx0 = m.gx0;
+    si.gy0 = m.gy0;
+    si.ginv = m.ginv;
+    si.gw = m.gw;
+    si.gh = m.gh;
+    si.ndegen = (int)m.degen.size();
+    return si;
+}
+
+// Mover constants of one scene (AgentsMover.h:162,222-224) and its agent grid:
+// cells at least 1.0625 collision distances wide and about four agents per
+// cell, at most 2048 per axis; cell ids continue from cell_base.
+ScenePar scene_par(const Device& d, const SceneInfo& si, int cell_base) {
+    ScenePar p{};
+    p.cd = si.radius * 2.5f;
+    p.cd2 = p.cd * p.cd;
+    p.arrive = FLT_EPSILON + si.radius;
+    p.speed = si.speed;
+    const double w = std::max(1e-3, (double)si.bx1 - si.bx0), h = std::max(1e-3, (double)si.by1 - si.by0);
+    double cell = std::max((double)p.cd * 1.0625, 1e-4);
+    cell = std::max(cell, std::sqrt(w * h / std::max(1.0, 4.0 * si.A)));
+    cell = std::max(cell, std::max(w, h) / 2048.0);
+    p.ax0 = si.bx0;
+    p.ay0 = si.by0;
+    p.ainv = (float)(1.0 / cell);
+    p.aw = std::max(1, (int)std::ceil(w / cell) + 1);
+    p.ah = std::max(1, (int)std::ceil(h / cell) + 1);
+    p.cell_base = cell_base;
+    p.loc.x0 = si.gx0;
+    p.loc.y0 = si.gy0;
+    p.loc.inv = si.ginv;
+    p.loc.w = si.gw;
+    p.loc.h = si.gh;
+    p.loc.start = d.gstart + si.gstart_off;
+    p.loc.list = d.glist + si.glist_off;
+    p.loc.degen = d.degen + si.degen_off;
+    p.loc.ndegen = si.ndegen;
+    p.loc.tri = d.tri + 3 * (size_t)si.node_base;
+    p.loc.n = si.n;
+    p.loc.base = si.node_base;
+    return p;
+}
+
 MoverParams mover_params(Context& c) {
     Device& d = c.dev;
     MoverParams p{};
@@ -113,45 +171,30 @@ MoverParams mover_params(Context& c) {
     p.path_len = d.path_len;
     p.paths = d.paths;
     p.path_stride = d.path_stride;
-    p.step = reinterpret_cast<const float*>(d.counters + 8);
-    p.cd = c.cfg.AgentRadius * 2.5f;  // AgentsMover.h:222
-    p.cd2 = p.cd * p.cd;
-    p.arrive = FLT_EPSILON + c.cfg.AgentRadius;  // AgentsMover.h:162,224
+    p.dt = reinterpret_cast<const float*>(d.counters + 8);
     // V2Float::GetRotated(10): cos/sin of 10 degrees, taken in double, rounded to float
     const double ang = 10.0 * 3.14159265358979323846 / 180.0;
     p.cs = (float)std::cos(ang);
     p.sn = (float)std::sin(ang);
-    const HostMap& m = c.map;
-    double w = std::max(1e-3, (double)m.bx1 - m.bx0), h = std::max(1e-3, (double)m.by1 - m.by0);
-    double cell = std::max((double)p.cd * 1.0625, 1e-4);
-    cell = std::max(cell, std::sqrt(w * h / std::max(1.0, 4.0 * c.A)));
-    cell = std::max(cell, std::max(w, h) / 2048.0);
-    p.ax0 = m.bx0;
-    p.ay0 = m.by0;
-    p.ainv = (float)(1.0 / cell);
-    p.aw = std::max(1, (int)std::ceil(w / cell) + 1);
-    p.ah = std::max(1, (int)std::ceil(h / cell) + 1);
+    p.sc = d.scene_par;
+    p.agent_scene = d.agent_scene;
+    p.cells = d.cells;
     p.cell_of = d.cell_of;
     p.cell_cnt = d.cell_cnt;
     p.cell_start = d.cell_start;
     p.cell_fill = d.cell_fill;
     p.cell_items = d.cell_items;
-    p.loc.x0 = m.gx0;
-    p.loc.y0 = m.gy0;
-    p.loc.inv = m.ginv;
-    p.loc.w = m.gw;
-    p.loc.h = m.gh;
-    p.loc.start = d.gstart;
-    p.loc.list = d.glist;
-    p.loc.degen = d.degen;
-    p.loc.ndegen = (int)m.degen.size();
-    p.loc.tri = d.tri;
-    p.loc.n = m.n;
+    p.tri = d.tri;
     p.cen = d.cen;
-    p.n = m.n;
+    p.n = c.map.n;
     p.stats = d.stats;
     p.err = d.counters + CT_ERR;
     return p;
+}
+
+CompactScenes compact_scenes(const Context& c) {
+    const Device& d = c.dev;
+    return CompactScenes{d.agent_scene, d.scene_abase, d.scene_P, d.scene_first};
 }
 
 int pick_slots(Context& c, int& blocks, std::string& err) {
@@ -252,7 +295,7 @@ int enqueue_frame(Context& c, bool timing, std::string& err) {
     cudaStream_t s = d.stream, s2 = d.stream2;
     if (timing) CK(cudaEventRecordWithFlags(d.ev[0], s, cudaEventRecordExternal));
     CK(cudaMemsetAsync(d.counters + CT_ERR, 0, sizeof(int), s));
-    launch_compact(s, c.A, d.state, d.cur, d.targ, c.cfg.PathFinderParallelAgents, d.req,
+    launch_compact(s, c.A, d.state, d.cur, d.targ, c.cfg.PathFinderParallelAgents, compact_scenes(c), d.req,
                    d.counters + CT_REQ, d.in_move, d.counters + CT_MOVE, d.counters + CT_WORK, d.stats);
     if (timing) CK(cudaEventRecordWithFlags(d.ev[1], s, cudaEventRecordExternal));
     CK(cudaEventRecord(d.ev[5], s));
@@ -321,6 +364,10 @@ int device_start(Context& c, std::string& err) {
 
     const HostMap& m = c.map;
     const int n = m.n;
+    if (c.scenes.empty()) c.scenes.push_back(single_scene(c));
+    const int nsc = (int)c.scenes.size();
+    int max_scene_n = 1;
+    for (const SceneInfo& si : c.scenes) max_scene_n = std::max(max_scene_n, si.n);
     // map
     DALLOC(d.rows, n);
     DALLOC(d.cen, n);
@@ -352,7 +399,7 @@ int device_start(Context& c, std::string& err) {
     DALLOC(d.in_move, A);
     DALLOC(d.dirty, A);
     d.dirty_cap = A;
-    d.path_stride = std::max(1, n);
+    d.path_stride = max_scene_n;  // a path holds at most its scene's triangles
     {
         size_t freeb = 0, totalb = 0;
         CK(cudaMemGetInfo(&freeb, &totalb));
@@ -366,7 +413,7 @@ int device_start(Context& c, std::string& err) {
     DALLOC(d.paths, (size_t)std::max(1, A) * d.path_stride);
     DALLOC(d.req, std::max(1, c.cfg.PathFinderParallelAgents));
     DALLOC(d.counters, CT_COUNT);
-    if (c.opt.order_by_estimate && c.opt.mode == GMAPF_MODE_BATCHED && n > 0) {
+    if (c.opt.order_by_estimate && c.opt.mode == GMAPF_MODE_BATCHED && n > 0 && nsc == 1) {
         // landmark hop distances for the longest-first request order
         std::vector<unsigned short> lm;
         d.lm_count = 8;
@@ -391,9 +438,32 @@ int device_start(Context& c, std::string& err) {
         CK(cudaMemcpy(d.step_node, minus.data(), sizeof(int) * A, cudaMemcpyHostToDevice));
     }
 
-    // agent grid
-    MoverParams mp = mover_params(c);
-    d.cells = mp.aw * mp.ah;
+    // scene table and agent grid
+    c.scene_par.clear();
+    d.cells = 0;
+    for (const SceneInfo& si : c.scenes) {
+        c.scene_par.push_back(scene_par(d, si, d.cells));
+        d.cells += c.scene_par.back().aw * c.scene_par.back().ah;
+    }
+    DALLOC(d.scene_par, nsc);
+    CK(cudaMemcpy(d.scene_par, c.scene_par.data(), sizeof(ScenePar) * nsc, cudaMemcpyHostToDevice));
+    if (nsc > 1) {
+        std::vector<int> as(std::max(1, A), 0), ab(nsc + 1, 0), sp(nsc, 0);
+        for (int s = 0; s < nsc; s++) {
+            const SceneInfo& si = c.scenes[s];
+            for (int i = 0; i < si.A; i++) as[si.agent_base + i] = s;
+            ab[s] = si.agent_base;
+            sp[s] = si.P;
+        }
+        ab[nsc] = A;
+        DALLOC(d.agent_scene, std::max(1, A));
+        DALLOC(d.scene_abase, nsc + 1);
+        DALLOC(d.scene_P, nsc);
+        DALLOC(d.scene_first, nsc);
+        CK(cudaMemcpy(d.agent_scene, as.data(), sizeof(int) * as.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.scene_abase, ab.data(), sizeof(int) * ab.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.scene_P, sp.data(), sizeof(int) * sp.size(), cudaMemcpyHostToDevice));
+    }
     DALLOC(d.cell_of, A);
     DALLOC(d.cell_cnt, (size_t)d.cells + 1);
     DALLOC(d.cell_start, (size_t)d.cells + 1);
@@ -455,7 +525,7 @@ int device_async_step(Context& c, float dt, std::string& err) {
         for (const int4& r : c.dirty_recs) c.dirty_slot[r.x] = -1;
         c.dirty_recs.clear();
     }
-    c.h_step[0] = c.cfg.AgentSpeed * dt;
+    c.h_step[0] = dt;  // each scene's step is speed * dt, rounded once (AgentsMover.h:63)
     CK(cudaMemcpyAsync(d.counters + 8, c.h_step, sizeof(float), cudaMemcpyHostToDevice, s));
 
     if (c.opt.mode == GMAPF_MODE_BATCHED) {
@@ -470,7 +540,7 @@ int device_async_step(Context& c, float dt, std::string& err) {
         const bool timing = c.cfg.IsProfiler != 0;
         if (timing) CK(cudaEventRecord(d.ev[0], s));
         CK(cudaMemsetAsync(d.counters + CT_ERR, 0, sizeof(int), s));
-        launch_compact(s, c.A, d.state, d.cur, d.targ, c.cfg.PathFinderParallelAgents, d.req,
+        launch_compact(s, c.A, d.state, d.cur, d.targ, c.cfg.PathFinderParallelAgents, compact_scenes(c), d.req,
                        d.counters + CT_REQ, d.in_move, d.counters + CT_MOVE, d.counters + CT_WORK,
                        d.stats);
         c.launches += 1;
@@ -589,12 +659,13 @@ int device_wait_step(Context& c, std::string& err) {
     return GMAPF_OK;
 }
 
-int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, std::string& err) {
+int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, int id_base,
+                              int id_count, std::string& err) {
     Device& d = c.dev;
     CK(cudaSetDevice(d.device));
-    MoverParams mp = mover_params(c);
-    launch_apply_targets_device(d.stream, d_ids, reinterpret_cast<const float2*>(d_pos), n, c.A, mp.loc, d.state,
-                                d.targ, d.targ_pos, d.counters + CT_ERR_TARGETS);
+    launch_apply_targets_device(d.stream, d_ids, reinterpret_cast<const float2*>(d_pos), n, id_base, id_count,
+                                d.scene_par, d.agent_scene, d.state, d.targ, d.targ_pos,
+                                d.counters + CT_ERR_TARGETS);
     c.launches += 1;
     CK(cudaGetLastError());
     return GMAPF_OK;

@@ -51,11 +51,12 @@ struct LocateGrid {
     float x0, y0, inv;
     int w, h;
     const int* start;   // w*h+1
-    const int* list;
+    const int* list;    // triangle ids local to this map
     const int* degen;
     int ndegen;
-    const float2* tri;  // 3 vertices per node
+    const float2* tri;  // 3 vertices per triangle of this map
     int n;
+    int base;           // added to a found id (first global id of this map in a scene batch)
 };
 
 __host__ __device__ inline float get_sign(float p1x, float p1y, float p2x, float p2y, float p3x,
@@ -92,7 +93,7 @@ __host__ __device__ inline bool gm_isfinite(float x) { return x - x == 0.0f; }
 
 __host__ __device__ inline int locate_linear(const LocateGrid& g, float px, float py) {
     for (int i = 0; i < g.n; i++)
-        if (point_in_tri(px, py, g.tri[3 * i], g.tri[3 * i + 1], g.tri[3 * i + 2])) return i;
+        if (point_in_tri(px, py, g.tri[3 * i], g.tri[3 * i + 1], g.tri[3 * i + 2])) return i + g.base;
     return -1;
 }
 
@@ -117,7 +118,7 @@ __host__ __device__ inline int locate(const LocateGrid& g, float px, float py) {
             break;
         }
     }
-    return best;
+    return best >= 0 ? best + g.base : -1;
 }
 
 }  // namespace gmapf_b200

@@ -25,6 +25,7 @@ LocateGrid HostMap::view() const {
     g.ndegen = (int)degen.size();
     g.tri = tri.data();
     g.n = n;
+    g.base = 0;
     return g;
 }
 

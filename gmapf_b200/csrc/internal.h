@@ -73,6 +73,18 @@ struct SearchParams {
     int* err;
 };
 
+// Per-scene constants of the mover and of point location: one entry for a
+// context with one map; a scene batch concatenates several maps (global
+// triangle ids) and several agent ranges.
+struct ScenePar {
+    float ax0, ay0, ainv;    // agent grid: origin, inverse cell size
+    int aw, ah, cell_base;   // cells per axis, first global cell
+    float cd, cd2;           // collision distance (2.5 r) and its square
+    float arrive;            // FLT_EPSILON + r
+    float speed;
+    LocateGrid loc;          // this scene's triangles (found ids are global)
+};
+
 struct MoverParams {
     int A;
     const int* mv_count;
@@ -88,20 +100,19 @@ struct MoverParams {
     const int* path_len;
     const int* paths;
     long long path_stride;
-    const float* step; // speed * dt (device scalar, set per frame)
-    float cd, cd2;     // collision distance and its square
-    float arrive;      // FLT_EPSILON + radius
+    const float* dt;   // frame dt (device scalar, set per frame); step = speed * dt
     float cs, sn;      // rotation by +10 degrees
-    // agent grid
-    float ax0, ay0, ainv;
-    int aw, ah;
+    const ScenePar* sc;        // per scene
+    const int* agent_scene;    // scene of each agent, or null (one scene)
+    // agent grid (all scenes' cells, global ids)
+    int cells;
     int* cell_of;
-    int* cell_cnt;     // aw*ah + 1
-    int* cell_start;   // aw*ah + 1
-    int* cell_fill;    // aw*ah
+    int* cell_cnt;     // cells + 1
+    int* cell_start;   // cells + 1
+    int* cell_fill;    // cells
     int* cell_items;   // A
     // map
-    LocateGrid loc;
+    const float2* tri; // 3 vertices per triangle, global ids
     const float2* cen;
     int n;
     unsigned long long* stats;
@@ -109,14 +120,24 @@ struct MoverParams {
 };
 
 // kernels.cu
+// Scene limits for compaction: agents of scene s are [abase[s], abase[s+1]);
+// at most P[s] requests per scene per frame, in ascending agent id.  All null
+// for a context with one map (P applies).  first: nscenes ints of scratch.
+struct CompactScenes {
+    const int* agent_scene;
+    const int* abase;
+    const int* P;
+    int* first;
+};
 void launch_compact(cudaStream_t s, int A, int* state, const int* cur, const int* targ, int P,
-                    int4* req, int* req_count, unsigned char* in_move, int* mv_count, int* work_ctr,
-                    unsigned long long* stats);
+                    const CompactScenes& scn, int4* req, int* req_count, unsigned char* in_move, int* mv_count,
+                    int* work_ctr, unsigned long long* stats);
 void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, int* targ_node,
                           float2* targ_pos);
-void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int A,
-                                 const LocateGrid& loc, int* state, int* targ_node, float2* targ_pos,
-                                 int* err);
+// device-resident retargets of agents id_base + ids[k], ids[k] in [0, id_count)
+void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int id_base,
+                                 int id_count, const ScenePar* sc, const int* agent_scene, int* state,
+                                 int* targ_node, float2* targ_pos, int* err);
 // requests reordered longest-first by the landmark estimate (keys: scratch, one int per request)
 void launch_order_requests(cudaStream_t s, const int4* req_in, const int* req_count, int4* req_out, int* keys,
                            const unsigned short* lm, int L, int n);
@@ -167,6 +188,20 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// One map with its agents inside a context: a plain context has exactly one
+// (the whole map and every agent); a scene batch's world has one per scene.
+struct SceneInfo {
+    int node_base = 0, n = 0;     // global triangle range
+    int agent_base = 0, A = 0;    // global agent range
+    int P = 0;                    // requests per frame (Config.PathFinderParallelAgents)
+    float radius = 0, speed = 0;
+    float bx0 = 0, by0 = 0, bx1 = 0, by1 = 0;  // map bounds (agent grid)
+    float gx0 = 0, gy0 = 0, ginv = 1;          // point-location grid
+    int gw = 1, gh = 1;
+    size_t gstart_off = 0, glist_off = 0, degen_off = 0;
+    int ndegen = 0;
+};
+
 struct Device {
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -205,6 +240,10 @@ struct Device {
     int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
         *cell_items = nullptr;
     int cells = 0;
+    // scenes (ScenePar per scene; the rest only when there is more than one)
+    ScenePar* scene_par = nullptr;
+    int* agent_scene = nullptr;
+    int *scene_abase = nullptr, *scene_P = nullptr, *scene_first = nullptr;
     // batch API scratch
     int4* breq = nullptr;
     int breq_cap = 0;
@@ -256,6 +295,10 @@ struct Context {
     float* h_step = nullptr;
     std::vector<int4> dirty_recs;
     std::vector<int> dirty_slot;       // agent -> index in dirty_recs or -1
+    // maps and agent ranges on the device (filled at start: one entry unless
+    // this context is a scene batch's world)
+    std::vector<SceneInfo> scenes;
+    std::vector<ScenePar> scene_par;  // host copy, device pointers inside
     // effective search parameters
     int T = 4, C = 16, block_threads = 128;
     float K = 1.0f;
@@ -287,7 +330,8 @@ int device_debug_agents(Context& c, gmapf_v2* pos, int* state, int* cur, int* ta
 int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::string& err);
 int device_autotune(Context& c, std::string& err);
 int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
-int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, std::string& err);
+int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, int id_base,
+                              int id_count, std::string& err);
 
 // capi.cpp: message returned by gmapf_last_error() on this thread
 void set_last_error(const std::string& msg);

@@ -23,16 +23,23 @@ namespace {
 
 constexpr int kCompactThreads = 1024;
 
+// Per-scene request limits (a scene batch): scene s takes its Search agents in
+// ascending id up to P[s] (each scene is its own PathFinder, PathFinder.h:76-117).
+// first[s] records how many Search agents precede the scene's first agent.
 __global__ void __launch_bounds__(kCompactThreads)
-    k_compact(int A, int* state, const int* cur, const int* targ, int P, int4* req, int* req_count,
-              unsigned char* in_move, int* mv_count, int* work_ctr, unsigned long long* stats) {
+    k_compact(int A, int* state, const int* cur, const int* targ, int P, CompactScenes scn, int4* req,
+              int* req_count, unsigned char* in_move, int* mv_count, int* work_ctr, unsigned long long* stats) {
     __shared__ int warp_tot[32];
     __shared__ int warp_totm[32];
-    __shared__ int base_s, base_m;
+    __shared__ int warp_toto[32];
+    __shared__ int base_s, base_m, base_o;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const bool scenes = scn.agent_scene != nullptr;
     if (tid == 0) {
         base_s = 0;
         base_m = 0;
+        base_o = 0;
     }
     __syncthreads();
     for (int b = 0; b < A; b += kCompactThreads) {
@@ -76,19 +83,39 @@ __global__ void __launch_bounds__(kCompactThreads)
         }
         __syncthreads();
         const int wpre = (warp == 0) ? 0 : warp_tot[warp - 1];
-        if (isS) {
-            const int pos = base_s + wpre + __popc(bs & ((1u << lane) - 1u));
-            if (pos < P) req[pos] = make_int4(i, cu, ta, i);  // over capacity: stays Search
+        const int gpos = base_s + wpre + __popc(bs & lt);  // Search agents before i
+        if (!scenes) {
+            if (isS && gpos < P) req[gpos] = make_int4(i, cu, ta, i);  // over capacity: stays Search
+        } else {
+            const int sidx = i < A ? scn.agent_scene[i] : 0;
+            if (i < A && i == scn.abase[sidx]) scn.first[sidx] = gpos;
+            __syncthreads();
+            const bool ok = isS && gpos - scn.first[sidx] < scn.P[sidx];
+            const unsigned bo = __ballot_sync(0xffffffffu, ok);
+            if (lane == 0) warp_toto[warp] = __popc(bo);
+            __syncthreads();
+            if (warp == 0) {
+                int v = warp_toto[lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    int t = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane >= o) v += t;
+                }
+                warp_toto[lane] = v;
+            }
+            __syncthreads();
+            const int opos = base_o + (warp == 0 ? 0 : warp_toto[warp - 1]) + __popc(bo & lt);
+            if (ok) req[opos] = make_int4(i, cu, ta, i);
         }
         __syncthreads();
         if (tid == 0) {
             base_s += warp_tot[31];
             base_m += warp_totm[31];
+            if (scenes) base_o += warp_toto[31];
         }
         __syncthreads();
     }
     if (tid == 0) {
-        const int R = base_s < P ? base_s : P;
+        const int R = scenes ? base_o : (base_s < P ? base_s : P);
         *req_count = R;
         *mv_count = base_m;
         *work_ctr = 0;
@@ -109,17 +136,19 @@ __global__ void k_apply_targets(const int4* recs, int n, int* state, int* targ_n
 
 // device-resident retargets: locate each target on the device (the host
 // path's CuNodesMap::TryGetNodeIdx rule) and mark the agent Search
-__global__ void k_apply_targets_device(const int* ids, const float2* pos, int n, int A, LocateGrid loc,
-                                       int* state, int* targ_node, float2* targ_pos, int* err) {
+__global__ void k_apply_targets_device(const int* ids, const float2* pos, int n, int id_base, int id_count,
+                                       const ScenePar* sc, const int* agent_scene, int* state, int* targ_node,
+                                       float2* targ_pos, int* err) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int id = ids[k];
+    const int lid = ids[k];
     const float2 p = pos[k];
-    if (id < 0 || id >= A) {
+    if (lid < 0 || lid >= id_count) {
         atomicOr(err, ERR_BAD_REQUEST);
         return;
     }
-    const int node = locate(loc, p.x, p.y);
+    const int id = id_base + lid;
+    const int node = locate(sc[agent_scene ? agent_scene[id] : 0].loc, p.x, p.y);
     if (node < 0) {
         atomicOr(err, ERR_BAD_REQUEST);
         return;
@@ -218,8 +247,9 @@ __global__ void k_move_bin(MoverParams p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (*p.mv_count == 0) return;  // AgentsMover.h:296-297
     if (i >= p.A) return;
+    const ScenePar& sc = p.sc[p.agent_scene ? p.agent_scene[i] : 0];
     float2 c = p.pos[i];
-    const float step = *p.step;
+    const float step = GM_FMUL(sc.speed, *p.dt);
     if (p.in_move[i] && p.step_idx[i] != -1) {
         const float2 s = p.step_pos[i];
         const float dx = GM_FSUB(s.x, c.x), dy = GM_FSUB(s.y, c.y);
@@ -234,9 +264,9 @@ __global__ void k_move_bin(MoverParams p) {
     p.pos_mid[i] = c;
     int cell = -1;
     if (gm_isfinite(c.x) && gm_isfinite(c.y)) {
-        const int cx = grid_cell(c.x, p.ax0, p.ainv, p.aw);
-        const int cy = grid_cell(c.y, p.ay0, p.ainv, p.ah);
-        cell = cy * p.aw + cx;
+        const int cx = grid_cell(c.x, sc.ax0, sc.ainv, sc.aw);
+        const int cy = grid_cell(c.y, sc.ay0, sc.ainv, sc.ah);
+        cell = sc.cell_base + cy * sc.aw + cx;
         atomicAdd(p.cell_cnt + cell, 1);
     }
     p.cell_of[i] = cell;
@@ -246,7 +276,7 @@ __global__ void k_move_bin(MoverParams p) {
 __global__ void __launch_bounds__(1024) k_cell_scan(MoverParams p) {
     if (*p.mv_count == 0) return;
     __shared__ int part[1024];
-    const int cells = p.aw * p.ah;
+    const int cells = p.cells;
     const int tid = threadIdx.x;
     const int per = (cells + 1023) / 1024;
     const int b = tid * per, e = min(b + per, cells);
@@ -286,33 +316,35 @@ __global__ void k_collide_progress(MoverParams p) {
     if (*p.mv_count == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.A) return;
+    const ScenePar& sc = p.sc[p.agent_scene ? p.agent_scene[i] : 0];
     const float2 me = p.pos_mid[i];
     float2 np = me;
     const int c = p.cell_of[i];
     if (c >= 0) {
-        const int cx = c % p.aw, cy = c / p.aw;
-        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, p.aw - 1);
-        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, p.ah - 1);
+        const int lc = c - sc.cell_base;  // cell within the agent's scene
+        const int cx = lc % sc.aw, cy = lc / sc.aw;
+        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, sc.aw - 1);
+        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, sc.ah - 1);
         int ids[kMaxLocal];
         float vxs[kMaxLocal], vys[kMaxLocal];
         int cnt = 0;
         bool overflow = false;
         for (int yy = y0; yy <= y1; yy++)
             for (int xx = x0; xx <= x1; xx++) {
-                const int cc = yy * p.aw + xx;
+                const int cc = sc.cell_base + yy * sc.aw + xx;
                 for (int k = p.cell_start[cc], e = p.cell_start[cc + 1]; k < e; k++) {
                     const int j = p.cell_items[k];
                     if (j == i) continue;
                     const float2 o = p.pos_mid[j];
                     const float dx = GM_FSUB(me.x, o.x), dy = GM_FSUB(me.y, o.y);
                     const float d2 = GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy));
-                    if (!(d2 < p.cd2)) continue;
+                    if (!(d2 < sc.cd2)) continue;
                     if (cnt >= kMaxLocal) {
                         overflow = true;
                         continue;
                     }
                     const float d = GM_FSQRT(d2);
-                    const float shift = GM_FSUB(p.cd, d);
+                    const float shift = GM_FSUB(sc.cd, d);
                     const float vx = GM_FMUL(GM_FDIV(dx, d), shift);
                     const float vy = GM_FMUL(GM_FDIV(dy, d), shift);
                     // insertion keeps ids ascending
@@ -344,16 +376,16 @@ __global__ void k_collide_progress(MoverParams p) {
                 float bvx = 0.f, bvy = 0.f;
                 for (int yy = y0; yy <= y1; yy++)
                     for (int xx = x0; xx <= x1; xx++) {
-                        const int cc = yy * p.aw + xx;
+                        const int cc = sc.cell_base + yy * sc.aw + xx;
                         for (int k = p.cell_start[cc], e = p.cell_start[cc + 1]; k < e; k++) {
                             const int j = p.cell_items[k];
                             if (j == i || j <= last || j >= best) continue;
                             const float2 o = p.pos_mid[j];
                             const float dx = GM_FSUB(me.x, o.x), dy = GM_FSUB(me.y, o.y);
                             const float d2 = GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy));
-                            if (!(d2 < p.cd2)) continue;
+                            if (!(d2 < sc.cd2)) continue;
                             const float d = GM_FSQRT(d2);
-                            const float shift = GM_FSUB(p.cd, d);
+                            const float shift = GM_FSUB(sc.cd, d);
                             best = j;
                             bvx = GM_FMUL(GM_FDIV(dx, d), shift);
                             bvy = GM_FMUL(GM_FDIV(dy, d), shift);
@@ -372,7 +404,7 @@ __global__ void k_collide_progress(MoverParams p) {
             const float rx = GM_FSUB(GM_FMUL(ax, p.cs), GM_FMUL(ay, p.sn));
             const float ry = GM_FADD(GM_FMUL(ax, p.sn), GM_FMUL(ay, p.cs));
             const float px = GM_FADD(me.x, rx), py = GM_FADD(me.y, ry);
-            if (locate(p.loc, px, py) >= 0) np = make_float2(px, py);
+            if (locate(sc.loc, px, py) >= 0) np = make_float2(px, py);
         }
     }
     p.pos[i] = np;
@@ -398,7 +430,7 @@ __global__ void k_collide_progress(MoverParams p) {
         atomicOr(p.err, ERR_BOUNDS);
         return;
     }
-    if (!point_in_tri(np.x, np.y, p.loc.tri[3 * sn], p.loc.tri[3 * sn + 1], p.loc.tri[3 * sn + 2]))
+    if (!point_in_tri(np.x, np.y, p.tri[3 * sn], p.tri[3 * sn + 1], p.tri[3 * sn + 2]))
         return;
     p.cur_node[i] = sn;
     if (si < L) si += 1;
@@ -407,7 +439,7 @@ __global__ void k_collide_progress(MoverParams p) {
         const float2 t = p.targ_pos[i];
         const float dx = GM_FSUB(t.x, np.x), dy = GM_FSUB(t.y, np.y);
         const float len = GM_FSQRT(GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy)));
-        if (len > p.arrive)
+        if (len > sc.arrive)
             p.step_pos[i] = t;
         else
             p.state[i] = GMAPF_AGENT_IDLE;
@@ -423,9 +455,9 @@ inline int blocks_for(int n, int bt) { return (n + bt - 1) / bt; }
 }  // namespace
 
 void launch_compact(cudaStream_t s, int A, int* state, const int* cur, const int* targ, int P,
-                    int4* req, int* req_count, unsigned char* in_move, int* mv_count, int* work_ctr,
-                    unsigned long long* stats) {
-    k_compact<<<1, kCompactThreads, 0, s>>>(A, state, cur, targ, P, req, req_count, in_move, mv_count,
+                    const CompactScenes& scn, int4* req, int* req_count, unsigned char* in_move, int* mv_count,
+                    int* work_ctr, unsigned long long* stats) {
+    k_compact<<<1, kCompactThreads, 0, s>>>(A, state, cur, targ, P, scn, req, req_count, in_move, mv_count,
                                             work_ctr, stats);
 }
 
@@ -435,12 +467,12 @@ void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, i
     k_apply_targets<<<blocks_for(n, 256), 256, 0, s>>>(recs, n, state, targ_node, targ_pos);
 }
 
-void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int A,
-                                 const LocateGrid& loc, int* state, int* targ_node, float2* targ_pos,
-                                 int* err) {
+void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int id_base,
+                                 int id_count, const ScenePar* sc, const int* agent_scene, int* state,
+                                 int* targ_node, float2* targ_pos, int* err) {
     if (n <= 0) return;
-    k_apply_targets_device<<<blocks_for(n, 256), 256, 0, s>>>(ids, pos, n, A, loc, state, targ_node, targ_pos,
-                                                              err);
+    k_apply_targets_device<<<blocks_for(n, 256), 256, 0, s>>>(ids, pos, n, id_base, id_count, sc, agent_scene,
+                                                              state, targ_node, targ_pos, err);
 }
 
 void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets, int n, int nodes,
