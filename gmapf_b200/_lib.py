@@ -120,6 +120,10 @@ SIGNATURES = {
     "gmapf_search_batch_device": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(StepStats)]),
     "gmapf_last_search_ms": (C.c_int, [P, C.POINTER(C.c_float)]),
+    "gmapf_batch_create": (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(Options), C.POINTER(P)]),
+    "gmapf_batch_destroy": (C.c_int, [P]),
+    "gmapf_batch_world": (P, [P]),
+    "gmapf_batch_scene_base": (C.c_int, [P, C.c_int32, I32P, I32P]),
     "gmapf_search_batch_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
                                              C.c_int32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                              C.c_void_p]),

@@ -59,6 +59,19 @@ def make_config(agents_max: int, radius: float, speed: float, parallel_agents: i
     return c
 
 
+def make_options(mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0, autotune: bool = False,
+                 search_mem_budget: int = 0, order_by_estimate: bool = True, visited_mode: int = 0) -> Options:
+    o = Options()
+    o.device = device
+    o.mode = mode
+    o.block_threads = block_threads
+    o.autotune = 1 if autotune else 0
+    o.search_mem_budget = search_mem_budget
+    o.order_by_estimate = 1 if order_by_estimate else 0
+    o.visited_mode = visited_mode
+    return o
+
+
 class GMAPF:
     """gmapf::GMAPF with the same lifecycle: Init -> FillMap* -> AddAgent ->
     (SetAgentTargPos) -> [ManualStart] -> AsyncStep/WaitStepEnd ..."""
@@ -68,6 +81,16 @@ class GMAPF:
         h = C.c_void_p()
         self._check(self._lib.gmapf_create(C.byref(h)))
         self._h = h
+        self._owned = True
+
+    @classmethod
+    def _view(cls, handle) -> "GMAPF":
+        """A non-owning wrapper (a scene batch's world)."""
+        g = cls.__new__(cls)
+        g._lib = _lib.load()
+        g._h = C.c_void_p(handle)
+        g._owned = False
+        return g
 
     # -- plumbing --------------------------------------------------------
     def _check(self, rc: int) -> None:
@@ -77,7 +100,8 @@ class GMAPF:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            self._lib.gmapf_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._lib.gmapf_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -143,17 +167,10 @@ class GMAPF:
         self._check(self._lib.gmapf_profiler_dump(self._h))
 
     # -- extras ------------------------------------------------------------
-    def set_options(self, mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0,
-                    autotune: bool = False, search_mem_budget: int = 0, order_by_estimate: bool = True,
-                    visited_mode: int = 0) -> None:
-        o = Options()
-        o.device = device
-        o.mode = mode
-        o.block_threads = block_threads
-        o.autotune = 1 if autotune else 0
-        o.search_mem_budget = search_mem_budget
-        o.order_by_estimate = 1 if order_by_estimate else 0
-        o.visited_mode = visited_mode
+    def set_options(self, **kw) -> None:
+        """mode, device, block_threads, autotune, search_mem_budget,
+        order_by_estimate, visited_mode (see gmapf_options)."""
+        o = make_options(**kw)
         self._check(self._lib.gmapf_set_options(self._h, C.byref(o)))
 
     def options(self) -> dict:
@@ -272,3 +289,53 @@ class GMAPF:
         v = C.c_float()
         self._check(self._lib.gmapf_last_search_ms(self._h, C.byref(v)))
         return v.value
+
+
+class SceneBatch:
+    """Several scenes stepped as one (gmapf_batch_*): each scene is a GMAPF
+    that was initialised, filled and given its agents; after binding, the
+    scenes keep their per-agent calls (SetAgentTargPos, GetAgentPos, ...)
+    with their own ids, and frames run on the batch (one compaction, one
+    persistent search launch and one mover pass for all scenes).  `world` is
+    the merged context (global agent and triangle ids) for statistics,
+    device-resident retargets and the stream handle."""
+
+    def __init__(self, scenes, **options):
+        self._lib = _lib.load()
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * len(self.scenes))(*[g._h.value for g in self.scenes])
+        h = C.c_void_p()
+        o = make_options(**options) if options else None
+        rc = self._lib.gmapf_batch_create(arr, len(self.scenes), C.byref(o) if o is not None else None, C.byref(h))
+        if rc != 0:
+            msg = self._lib.gmapf_last_error()
+            raise GMAPFError(rc, msg.decode() if msg else "")
+        self._h = h
+        self.world = GMAPF._view(self._lib.gmapf_batch_world(h))
+
+    def scene_base(self, scene: int):
+        """(first global agent id, first global triangle id) of a scene."""
+        a, n = C.c_int32(), C.c_int32()
+        self.world._check(self._lib.gmapf_batch_scene_base(self._h, int(scene), C.byref(a), C.byref(n)))
+        return a.value, n.value
+
+    def ManualStart(self) -> None:
+        self.world.ManualStart()
+
+    def AsyncStep(self, dt: float) -> None:
+        self.world.AsyncStep(dt)
+
+    def WaitStepEnd(self) -> None:
+        self.world.WaitStepEnd()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self.world._h = None
+            self._lib.gmapf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

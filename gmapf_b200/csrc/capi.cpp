@@ -11,8 +11,17 @@
 
 using namespace gmapf_b200;
 
+struct gmapf_batch;
+
 struct gmapf_ctx {
     Context c;
+    gmapf_batch* batch = nullptr;  // the batch this scene is bound to
+    gmapf_ctx* world = nullptr;    // that batch's world
+};
+
+struct gmapf_batch {
+    gmapf_ctx* world = nullptr;
+    std::vector<gmapf_ctx*> scenes;
 };
 
 namespace {
@@ -26,6 +35,16 @@ gmapf_status fail(int code, const std::string& msg) {
 
 #define NEED_CTX(ctx) \
     if (!(ctx)) return fail(GMAPF_E_INVALID_ARG, "null context")
+
+// A scene bound to a batch: its agent calls go to the world (null if the
+// scene is not bound); a scene whose batch was destroyed answers E_STATE.
+#define SCENE_WORLD(ctx, w)                                                                  \
+    if ((ctx)->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");   \
+    gmapf_ctx* w = (ctx)->world
+
+gmapf_status scene_only(const char* what) {
+    return fail(GMAPF_E_STATE, std::string(what) + ": this scene is stepped by its batch (use the batch's world)");
+}
 
 // PathFinder threads per agent: the reference packs 128/T requests per block
 // (PathFinder.h:559-572) and seeds lanes 0 and 1 (PathFinder.h:168-189).
@@ -98,7 +117,12 @@ gmapf_status gmapf_create(gmapf_ctx** out) {
 gmapf_status gmapf_destroy(gmapf_ctx* ctx) {
     if (!ctx) return GMAPF_OK;
     Context& c = ctx->c;
-    if (c.started) {
+    if (c.is_world) return fail(GMAPF_E_STATE, "the world context belongs to its batch: destroy the batch");
+    if (ctx->batch) {
+        auto& v = ctx->batch->scenes;
+        v.erase(std::remove(v.begin(), v.end(), ctx), v.end());
+    }
+    if (c.started && c.scene_index < 0) {  // a batch's scene holds no device state
         if (c.step_going) {
             std::string err;
             device_wait_step(c, err);
@@ -234,6 +258,7 @@ gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id) 
     Context& c = ctx->c;
     // src/GMAPF.cu:219-236
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.is_world) return fail(GMAPF_E_STATE, "agents are added to the scene contexts");
     if (c.started) return fail(GMAPF_E_STATE, "cannot add agents after start");
     if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
     if (c.A >= c.cfg.AgentsMaxCount) return fail(GMAPF_E_CAPACITY, "AgentsMaxCount reached");
@@ -253,6 +278,21 @@ gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id) 
 gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t id, float x, float y) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    SCENE_WORLD(ctx, w);
+    if (c.is_world)
+        return fail(GMAPF_E_STATE, "targets are set through the scene contexts (or gmapf_set_agent_targ_pos_device)");
+    if (w) {
+        if (id < 0 || id >= c.A) return fail(GMAPF_E_INVALID_ARG, "agent id " + std::to_string(id) + " out of range");
+        const int node = locate_host(c, x, y);
+        if (node < 0) return fail(GMAPF_E_INVALID_POS, "target pos " + v2s(x, y) + " is invalid");
+        Context& wc = w->c;
+        const int gid = c.agent_base + id, gnode = c.node_base + node;
+        wc.m_state[gid] = GMAPF_AGENT_SEARCH;
+        wc.m_targ[gid] = gmapf_v2{x, y};
+        wc.m_targ_node[gid] = gnode;
+        if (wc.started) add_dirty(wc, gid, gnode, x, y);
+        return GMAPF_OK;
+    }
     // src/GMAPF.cu:238-253
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
     if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
@@ -279,13 +319,16 @@ gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, c
 gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_ids, const gmapf_v2* d_pos,
                                              int32_t n) {
     NEED_CTX(ctx);
-    Context& c = ctx->c;
+    SCENE_WORLD(ctx, w);
+    // a bound scene's ids are its own: offset into the world's agents
+    Context& c = w ? w->c : ctx->c;
+    const int id_base = w ? ctx->c.agent_base : 0, id_count = w ? ctx->c.A : c.A;
     if (!c.started) return fail(GMAPF_E_STATE, "not started");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
     if (n < 0 || (n > 0 && (!d_ids || !d_pos))) return fail(GMAPF_E_INVALID_ARG, "bad device arrays");
     if (n == 0) return GMAPF_OK;
     std::string err;
-    int rc = device_set_targets_device(c, d_ids, d_pos, n, 0, c.A, err);
+    int rc = device_set_targets_device(c, d_ids, d_pos, n, id_base, id_count, err);
     if (rc) return fail(rc, err);
     return GMAPF_OK;
 }
@@ -293,6 +336,7 @@ gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_id
 gmapf_status gmapf_manual_start(gmapf_ctx* ctx) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    if (ctx->world || c.detached) return scene_only("ManualStart");
     // src/GMAPF.cu:72-130
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
     if (c.started) return fail(GMAPF_E_STATE, "already started");
@@ -302,6 +346,7 @@ gmapf_status gmapf_manual_start(gmapf_ctx* ctx) {
 gmapf_status gmapf_async_step(gmapf_ctx* ctx, float dt) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    if (ctx->world || c.detached) return scene_only("AsyncStep");
     // src/GMAPF.cu:255-289
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
     if (c.step_going) return GMAPF_OK;
@@ -317,6 +362,7 @@ gmapf_status gmapf_async_step(gmapf_ctx* ctx, float dt) {
 gmapf_status gmapf_wait_step_end(gmapf_ctx* ctx) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    if (ctx->world || c.detached) return scene_only("WaitStepEnd");
     // src/GMAPF.cu:291-314
     if (!c.step_going) return GMAPF_OK;
     std::string err;
@@ -329,27 +375,36 @@ gmapf_status gmapf_wait_step_end(gmapf_ctx* ctx) {
 gmapf_status gmapf_get_agent_pos(gmapf_ctx* ctx, int32_t id, gmapf_v2* out) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    SCENE_WORLD(ctx, w);
     if (id < 0 || id >= c.A || !out) return fail(GMAPF_E_INVALID_ARG, "agent id out of range");
-    *out = c.m_pos[id];
+    *out = w ? w->c.m_pos[c.agent_base + id] : c.m_pos[id];
     return GMAPF_OK;
 }
 
 gmapf_status gmapf_get_agent_state(gmapf_ctx* ctx, int32_t id, int32_t* out) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    SCENE_WORLD(ctx, w);
     if (id < 0 || id >= c.A || !out) return fail(GMAPF_E_INVALID_ARG, "agent id out of range");
-    *out = c.m_state[id];
+    *out = w ? w->c.m_state[c.agent_base + id] : c.m_state[id];
     return GMAPF_OK;
 }
 
-const gmapf_v2* gmapf_agent_pos_view(gmapf_ctx* ctx) { return ctx ? ctx->c.m_pos.data() : nullptr; }
+const gmapf_v2* gmapf_agent_pos_view(gmapf_ctx* ctx) {
+    if (!ctx || ctx->c.detached) return nullptr;
+    if (ctx->world) return ctx->world->c.m_pos.data() + ctx->c.agent_base;
+    return ctx->c.m_pos.data();
+}
 
 gmapf_status gmapf_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* state, int32_t n) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    SCENE_WORLD(ctx, w);
     if (n < 0 || n > c.A) return fail(GMAPF_E_INVALID_ARG, "n out of range");
-    if (pos) std::memcpy(pos, c.m_pos.data(), sizeof(gmapf_v2) * n);
-    if (state) std::memcpy(state, c.m_state.data(), sizeof(int32_t) * n);
+    const Context& src = w ? w->c : c;
+    const int b = w ? c.agent_base : 0;
+    if (pos) std::memcpy(pos, src.m_pos.data() + b, sizeof(gmapf_v2) * n);
+    if (state) std::memcpy(state, src.m_state.data() + b, sizeof(int32_t) * n);
     return GMAPF_OK;
 }
 
@@ -357,6 +412,8 @@ int32_t gmapf_agent_count(gmapf_ctx* ctx) { return ctx ? ctx->c.A : 0; }
 
 gmapf_status gmapf_profiler_dump(gmapf_ctx* ctx) {
     NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) ctx = ctx->world;
     Context& c = ctx->c;
     // src/GMAPF.cu:326-356, same line format
     if (!c.cfg.IsProfiler) return fail(GMAPF_E_STATE, "profiler disabled");
@@ -391,6 +448,7 @@ gmapf_status gmapf_get_map_nodes(gmapf_ctx* ctx, gmapf_node* out, int32_t cap) {
 gmapf_status gmapf_locate_points(gmapf_ctx* ctx, const gmapf_v2* pts, int32_t n, int32_t* out) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    if (c.is_world) return fail(GMAPF_E_STATE, "points are located in the scene contexts");
     if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
     if (n < 0 || (n > 0 && (!pts || !out))) return fail(GMAPF_E_INVALID_ARG, "bad arrays");
     LocateGrid g = c.map.view();
@@ -402,6 +460,32 @@ gmapf_status gmapf_debug_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* stat
                                     int32_t* targ, int32_t* step_idx, int32_t* step_node,
                                     gmapf_v2* step_pos, int32_t* path_len) {
     NEED_CTX(ctx);
+    SCENE_WORLD(ctx, w);
+    if (w) {  // the world's arrays, this scene's slice, triangle ids made local
+        Context& wc = w->c;
+        const Context& c = ctx->c;
+        if (!wc.started) return fail(GMAPF_E_STATE, "not started");
+        if (wc.step_going) return fail(GMAPF_E_STATE, "a step is running");
+        const int WA = wc.A, b = c.agent_base, A = c.A, nb = c.node_base;
+        std::vector<gmapf_v2> p(WA), sp(WA);
+        std::vector<int32_t> st(WA), cu(WA), tg(WA), si(WA), sn(WA), pl(WA);
+        std::string err;
+        int rc = device_debug_agents(wc, p.data(), st.data(), cu.data(), tg.data(), si.data(), sn.data(), sp.data(),
+                                     pl.data(), err);
+        if (rc) return fail(rc, err);
+        auto local = [nb](int v) { return v >= 0 ? v - nb : v; };
+        for (int i = 0; i < A; i++) {
+            if (pos) pos[i] = p[b + i];
+            if (state) state[i] = st[b + i];
+            if (cur) cur[i] = local(cu[b + i]);
+            if (targ) targ[i] = local(tg[b + i]);
+            if (step_idx) step_idx[i] = si[b + i];
+            if (step_node) step_node[i] = local(sn[b + i]);
+            if (step_pos) step_pos[i] = sp[b + i];
+            if (path_len) path_len[i] = pl[b + i];
+        }
+        return GMAPF_OK;
+    }
     Context& c = ctx->c;
     if (!c.started) return fail(GMAPF_E_STATE, "not started");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
@@ -413,18 +497,23 @@ gmapf_status gmapf_debug_get_agents(gmapf_ctx* ctx, gmapf_v2* pos, int32_t* stat
 
 gmapf_status gmapf_debug_get_path(gmapf_ctx* ctx, int32_t id, int32_t* out, int32_t cap, int32_t* out_len) {
     NEED_CTX(ctx);
-    Context& c = ctx->c;
+    SCENE_WORLD(ctx, w);
+    Context& c = w ? w->c : ctx->c;
     if (!c.started) return fail(GMAPF_E_STATE, "not started");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
-    if (id < 0 || id >= c.A || !out_len || (cap > 0 && !out)) return fail(GMAPF_E_INVALID_ARG, "bad arguments");
+    if (id < 0 || id >= ctx->c.A || !out_len || (cap > 0 && !out)) return fail(GMAPF_E_INVALID_ARG, "bad arguments");
     std::string err;
-    int rc = device_debug_path(c, id, out, cap, out_len, err);
+    int rc = device_debug_path(c, w ? ctx->c.agent_base + id : id, out, cap, out_len, err);
     if (rc) return fail(rc, err);
+    if (w)  // scene-local triangle ids
+        for (int k = 0; k < std::min(*out_len, cap); k++) out[k] -= ctx->c.node_base;
     return GMAPF_OK;
 }
 
 gmapf_status gmapf_last_step_stats(gmapf_ctx* ctx, gmapf_step_stats* out) {
     NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) ctx = ctx->world;
     if (!out) return fail(GMAPF_E_INVALID_ARG, "null output");
     *out = ctx->c.last;
     return GMAPF_OK;
@@ -432,6 +521,8 @@ gmapf_status gmapf_last_step_stats(gmapf_ctx* ctx, gmapf_step_stats* out) {
 
 gmapf_status gmapf_step_time_percentile(gmapf_ctx* ctx, float q, float* out_ms) {
     NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) ctx = ctx->world;
     if (!out_ms || q < 0 || q > 100) return fail(GMAPF_E_INVALID_ARG, "bad arguments");
     std::vector<float> v = ctx->c.prof.wall_ms;
     if (v.empty()) {
@@ -449,13 +540,19 @@ gmapf_status gmapf_step_time_percentile(gmapf_ctx* ctx, float q, float* out_ms) 
 
 gmapf_status gmapf_reset_profiler(gmapf_ctx* ctx) {
     NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) ctx = ctx->world;
     ctx->c.prof = Profiler{};
     return GMAPF_OK;
 }
 
-int64_t gmapf_kernel_launches(gmapf_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+int64_t gmapf_kernel_launches(gmapf_ctx* ctx) {
+    if (ctx && ctx->world) ctx = ctx->world;
+    return ctx ? ctx->c.launches : 0;
+}
 
 void* gmapf_stream_handle(gmapf_ctx* ctx) {
+    if (ctx && ctx->world) ctx = ctx->world;
     if (!ctx || !ctx->c.started) return nullptr;
     return (void*)ctx->c.dev.stream;
 }
@@ -463,6 +560,8 @@ void* gmapf_stream_handle(gmapf_ctx* ctx) {
 gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t* bt, int32_t* vm,
                                 int32_t* slots) {
     NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) ctx = ctx->world;
     Context& c = ctx->c;
     if (!c.started) return fail(GMAPF_E_STATE, "not started");
     if (T) *T = c.T;
@@ -478,6 +577,7 @@ gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, 
                                        int32_t path_stride, gmapf_step_stats* stats) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    if (ctx->world || c.detached) return scene_only("search batch");
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
     if (n < 0 || path_stride < 1) return fail(GMAPF_E_INVALID_ARG, "bad sizes");
@@ -496,6 +596,7 @@ gmapf_status gmapf_search_batch_host(gmapf_ctx* ctx, const int32_t* starts, cons
                                      int32_t path_stride, gmapf_step_stats* stats) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
+    if (ctx->world || c.detached) return scene_only("search batch");
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
     if (n < 0 || path_stride < 1) return fail(GMAPF_E_INVALID_ARG, "bad sizes");
@@ -532,8 +633,155 @@ gmapf_status gmapf_search_batch_host(gmapf_ctx* ctx, const int32_t* starts, cons
 
 gmapf_status gmapf_last_search_ms(gmapf_ctx* ctx, float* out_ms) {
     NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) ctx = ctx->world;
     if (!out_ms) return fail(GMAPF_E_INVALID_ARG, "null output");
     *out_ms = ctx->c.last_search_ms;
+    return GMAPF_OK;
+}
+
+// ------------------------------------------------------------ scene batches --
+
+gmapf_status gmapf_batch_create(gmapf_ctx* const* scenes, int32_t n, const gmapf_options* opt, gmapf_batch** out) {
+    if (!out) return fail(GMAPF_E_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    if (n < 1 || !scenes) return fail(GMAPF_E_INVALID_ARG, "a batch needs at least one scene");
+    for (int s = 0; s < n; s++) {
+        gmapf_ctx* sc = scenes[s];
+        const std::string who = "scene " + std::to_string(s);
+        if (!sc) return fail(GMAPF_E_INVALID_ARG, who + " is null");
+        for (int t = 0; t < s; t++)
+            if (scenes[t] == sc) return fail(GMAPF_E_INVALID_ARG, who + " is listed twice");
+        const Context& c = sc->c;
+        if (c.is_world) return fail(GMAPF_E_INVALID_ARG, who + " is a batch's world");
+        if (sc->world || c.detached) return fail(GMAPF_E_STATE, who + " already belongs to a batch");
+        if (!c.inited) return fail(GMAPF_E_STATE, who + " is not initialized");
+        if (!c.map_filled) return fail(GMAPF_E_STATE, who + " has no map");
+        if (c.started) return fail(GMAPF_E_STATE, who + " is already started");
+        const Context& c0 = scenes[0]->c;
+        if (c.T != c0.T || c.C != c0.C || c.K != c0.K)
+            return fail(GMAPF_E_INVALID_ARG, who + ": threads per agent, queue capacity and heuristic K must equal "
+                                                   "scene 0's (they shape the one search launch)");
+    }
+    if (opt) {
+        if (opt->mode != GMAPF_MODE_BATCHED && opt->mode != GMAPF_MODE_PLAIN)
+            return fail(GMAPF_E_INVALID_ARG, "unknown mode");
+        if (opt->block_threads != 0 &&
+            (opt->block_threads < 32 || opt->block_threads > 256 || opt->block_threads % 32 != 0))
+            return fail(GMAPF_E_INVALID_ARG, "block_threads must be 0 or a multiple of 32 in [32, 256]");
+        if (opt->visited_mode < 0 || opt->visited_mode > 3)
+            return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
+        if (opt->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
+    }
+    gmapf_batch* b = new (std::nothrow) gmapf_batch();
+    gmapf_ctx* w = new (std::nothrow) gmapf_ctx();
+    if (!b || !w) {
+        delete b;
+        delete w;
+        return fail(GMAPF_E_CAPACITY, "out of host memory");
+    }
+    Context& wc = w->c;
+    const Context& c0 = scenes[0]->c;
+    wc.is_world = true;
+    wc.opt.device = 0;
+    wc.opt.mode = GMAPF_MODE_BATCHED;
+    wc.opt.order_by_estimate = 1;
+    if (opt) wc.opt = *opt;
+    if (wc.opt.block_threads) wc.block_threads = wc.opt.block_threads;
+    // world map and scene table
+    std::vector<const HostMap*> maps;
+    for (int s = 0; s < n; s++) maps.push_back(&scenes[s]->c.map);
+    concat_host_maps(maps, wc.map, wc.scenes);
+    // world config: the search shape of the scenes, summed capacities
+    wc.cfg = c0.cfg;
+    wc.cfg.AgentsMaxCount = 0;
+    wc.cfg.PathFinderParallelAgents = 0;
+    wc.cfg.IsDebug = 0;
+    wc.cfg.IsProfiler = 0;
+    int A = 0;
+    for (int s = 0; s < n; s++) {
+        const Context& c = scenes[s]->c;
+        SceneInfo& si = wc.scenes[s];
+        si.agent_base = A;
+        si.A = c.A;
+        si.P = c.cfg.PathFinderParallelAgents;
+        si.radius = c.cfg.AgentRadius;
+        si.speed = c.cfg.AgentSpeed;
+        wc.cfg.AgentsMaxCount += c.A;
+        wc.cfg.PathFinderParallelAgents += std::min(c.cfg.PathFinderParallelAgents, std::max(c.A, 1));
+        wc.cfg.IsDebug |= c.cfg.IsDebug;
+        wc.cfg.IsProfiler |= c.cfg.IsProfiler;
+        A += c.A;
+    }
+    wc.T = c0.T;
+    wc.C = c0.C;
+    wc.K = c0.K;
+    // world agents: the scenes' agents one after another, triangle ids made global
+    wc.m_pos.reserve(A);
+    wc.m_state.reserve(A);
+    wc.m_cur.reserve(A);
+    wc.m_targ.reserve(A);
+    wc.m_targ_node.reserve(A);
+    for (int s = 0; s < n; s++) {
+        const Context& c = scenes[s]->c;
+        const int nb = wc.scenes[s].node_base;
+        for (int i = 0; i < c.A; i++) {
+            wc.m_pos.push_back(c.m_pos[i]);
+            wc.m_state.push_back(c.m_state[i]);
+            wc.m_cur.push_back(c.m_cur[i] >= 0 ? c.m_cur[i] + nb : -1);
+            wc.m_targ.push_back(c.m_targ[i]);
+            wc.m_targ_node.push_back(c.m_targ_node[i] >= 0 ? c.m_targ_node[i] + nb : -1);
+        }
+    }
+    wc.dirty_slot.assign(A, -1);
+    wc.A = A;
+    wc.inited = true;
+    wc.map_filled = true;
+    // bind the scenes
+    for (int s = 0; s < n; s++) {
+        gmapf_ctx* sc = scenes[s];
+        sc->batch = b;
+        sc->world = w;
+        sc->c.scene_index = s;
+        sc->c.agent_base = wc.scenes[s].agent_base;
+        sc->c.node_base = wc.scenes[s].node_base;
+        sc->c.started = true;  // no more map, agent or option changes
+        b->scenes.push_back(sc);
+    }
+    b->world = w;
+    *out = b;
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_batch_destroy(gmapf_batch* b) {
+    if (!b) return GMAPF_OK;
+    for (gmapf_ctx* sc : b->scenes) {
+        sc->batch = nullptr;
+        sc->world = nullptr;
+        sc->c.detached = true;
+    }
+    Context& wc = b->world->c;
+    if (wc.started) {
+        if (wc.step_going) {
+            std::string err;
+            device_wait_step(wc, err);
+            wc.step_going = false;
+        }
+        device_free(wc);
+    }
+    delete b->world;
+    delete b;
+    return GMAPF_OK;
+}
+
+gmapf_ctx* gmapf_batch_world(gmapf_batch* b) { return b ? b->world : nullptr; }
+
+gmapf_status gmapf_batch_scene_base(gmapf_batch* b, int32_t scene, int32_t* agent_base, int32_t* node_base) {
+    if (!b) return fail(GMAPF_E_INVALID_ARG, "null batch");
+    const Context& wc = b->world->c;
+    if (scene < 0 || scene >= (int)wc.scenes.size()) return fail(GMAPF_E_INVALID_ARG, "scene out of range");
+    if (agent_base) *agent_base = wc.scenes[scene].agent_base;
+    if (node_base) *node_base = wc.scenes[scene].node_base;
     return GMAPF_OK;
 }
 

@@ -188,4 +188,61 @@ void landmark_distances(const HostMap& m, int count, std::vector<unsigned short>
     }
 }
 
+void concat_host_maps(const std::vector<const HostMap*>& maps, HostMap& out, std::vector<SceneInfo>& scenes) {
+    out = HostMap{};
+    scenes.assign(maps.size(), SceneInfo{});
+    int base = 0;
+    float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY;
+    for (size_t s = 0; s < maps.size(); s++) {
+        const HostMap& m = *maps[s];
+        SceneInfo& si = scenes[s];
+        si.node_base = base;
+        si.n = m.n;
+        si.bx0 = m.bx0;
+        si.by0 = m.by0;
+        si.bx1 = m.bx1;
+        si.by1 = m.by1;
+        si.gx0 = m.gx0;
+        si.gy0 = m.gy0;
+        si.ginv = m.ginv;
+        si.gw = m.gw;
+        si.gh = m.gh;
+        si.gstart_off = out.gstart.size();
+        si.glist_off = out.glist.size();
+        si.degen_off = out.degen.size();
+        si.ndegen = (int)m.degen.size();
+        // grid cell lists keep scene-local ids: the scene's LocateGrid adds node_base
+        out.gstart.insert(out.gstart.end(), m.gstart.begin(), m.gstart.end());
+        out.glist.insert(out.glist.end(), m.glist.begin(), m.glist.end());
+        out.degen.insert(out.degen.end(), m.degen.begin(), m.degen.end());
+        for (int i = 0; i < m.n; i++) {
+            gmapf_node nd = m.nodes[i];
+            for (int k = 0; k < 3; k++)
+                if (nd.NeibsIdx[k] >= 0) nd.NeibsIdx[k] += base;
+            out.nodes.push_back(nd);
+            SearchRow r = m.rows[i];
+            if (r.n0 >= 0) r.n0 += base;
+            if (r.n1 >= 0) r.n1 += base;
+            if (r.n2 >= 0) r.n2 += base;
+            out.rows.push_back(r);
+            out.cen.push_back(m.cen[i]);
+            for (int k = 0; k < 3; k++) out.tri.push_back(m.tri[3 * (size_t)i + k]);
+        }
+        x0 = std::min(x0, m.bx0);
+        y0 = std::min(y0, m.by0);
+        x1 = std::max(x1, m.bx1);
+        y1 = std::max(y1, m.by1);
+        base += m.n;
+    }
+    out.n = base;
+    out.bx0 = x0;
+    out.by0 = y0;
+    out.bx1 = x1;
+    out.by1 = y1;
+    // the world has no single point-location grid: locating goes through the scenes
+    out.gx0 = out.gy0 = 0;
+    out.ginv = 1;
+    out.gw = out.gh = 1;
+}
+
 }  // namespace gmapf_b200

@@ -161,6 +161,20 @@ int search_max_blocks_per_sm(int T, int C, int block_threads, int vm, int bm_wor
 
 // ------------------------------------------------------------------- host --
 
+// One map with its agents inside a context: a plain context has exactly one
+// (the whole map and every agent); a scene batch's world has one per scene.
+struct SceneInfo {
+    int node_base = 0, n = 0;     // global triangle range
+    int agent_base = 0, A = 0;    // global agent range
+    int P = 0;                    // requests per frame (Config.PathFinderParallelAgents)
+    float radius = 0, speed = 0;
+    float bx0 = 0, by0 = 0, bx1 = 0, by1 = 0;  // map bounds (agent grid)
+    float gx0 = 0, gy0 = 0, ginv = 1;          // point-location grid
+    int gw = 1, gh = 1;
+    size_t gstart_off = 0, glist_off = 0, degen_off = 0;
+    int ndegen = 0;
+};
+
 struct HostMap {
     int n = 0;
     std::vector<gmapf_node> nodes;  // as ingested, PCenter recomputed
@@ -176,6 +190,10 @@ struct HostMap {
 
 // hostmap.cpp
 void build_host_map(const gmapf_node* nodes, int n, HostMap& out);
+// The world map of a scene batch: the scenes' maps one after another with
+// global triangle ids; fills each scene's triangle range, bounds and
+// point-location grid (offsets into the concatenated grid arrays).
+void concat_host_maps(const std::vector<const HostMap*>& maps, HostMap& out, std::vector<SceneInfo>& scenes);
 // Hop distances from `count` landmark triangles chosen by farthest-point
 // sampling over the neighbour graph (unreachable: 65535), count * n values.
 void landmark_distances(const HostMap& m, int count, std::vector<unsigned short>& out);
@@ -186,20 +204,6 @@ int build_navmesh_cdt(const std::vector<float>& verts, const std::vector<unsigne
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
-};
-
-// One map with its agents inside a context: a plain context has exactly one
-// (the whole map and every agent); a scene batch's world has one per scene.
-struct SceneInfo {
-    int node_base = 0, n = 0;     // global triangle range
-    int agent_base = 0, A = 0;    // global agent range
-    int P = 0;                    // requests per frame (Config.PathFinderParallelAgents)
-    float radius = 0, speed = 0;
-    float bx0 = 0, by0 = 0, bx1 = 0, by1 = 0;  // map bounds (agent grid)
-    float gx0 = 0, gy0 = 0, ginv = 1;          // point-location grid
-    int gw = 1, gh = 1;
-    size_t gstart_off = 0, glist_off = 0, degen_off = 0;
-    int ndegen = 0;
 };
 
 struct Device {
@@ -314,6 +318,12 @@ struct Context {
     bool pre_done = false;
     long long launches = 0;
     float last_search_ms = 0;
+    // scene batches: a scene context bound to a batch forwards its agent calls
+    // to the batch's world (agents [agent_base, agent_base + A), triangles
+    // [node_base, node_base + map.n) there)
+    int scene_index = -1, agent_base = 0, node_base = 0;
+    bool is_world = false;   // the merged context of a batch
+    bool detached = false;   // its batch was destroyed
     int plain_req_count = 0, plain_mv_count = 0;
 };
 

@@ -6,6 +6,8 @@ configurations (no dataset ships with the reference; these stand in for it).
         every agent retargeted every 100 steps
   cfg3  4000x4000 maze from a randomized-DFS maze of cells x cells (walls 4 wide),
         16384 agents, r=2, all retargeted in the same frame
+  cfg4  64 independent scenes of random sizes, obstacles, agent counts and radii
+        (a scene batch), retargets with probability 0.02 per agent per step
   zigzag  the reference driver's map (main.cpp:152-175) with its agent layout
         (main.cpp:14-43)
 
@@ -136,6 +138,27 @@ def cfg3(cells: int = 160, seed: int = 3, agents: int = 16384, threads_per_agent
     return Scenario(f"cfg3-maze{cells}", (4000.0, 4000.0), maze_walls(cells, 4000.0, 4.0, seed), agents=agents,
                     radius=2.0, speed=1.0, parallel_agents=agents, threads_per_agent=threads_per_agent,
                     queue_capacity=queue_capacity, steps=1, seed=seed, meta={"cells": cells})
+
+
+def cfg4(n_scenes: int = 64, seed: int = 4, agents_range=(64, 1024), threads_per_agent: int = 8,
+         queue_capacity: int = 32) -> list:
+    """The multi-scene configuration: n_scenes independent scenes, each with a
+    map side U[200, 2000], U[10, 500] rectangles with sides U[10, 60] (as many
+    as fit without overlap), U[agents_range] agents of radius U[1, 3] and speed
+    1, and random retargets with probability 0.02 per agent per step."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        side = float(rng.uniform(200, 2000))
+        nrect = int(rng.integers(10, 501))
+        A = int(rng.integers(agents_range[0], agents_range[1] + 1))
+        r = float(np.float32(rng.uniform(1, 3)))
+        sub = np.random.default_rng(int(rng.integers(1 << 30)))
+        out.append(Scenario(f"cfg4-scene{k}", (side, side), random_rects(sub, side, side, nrect, 10, 60, 20000),
+                            agents=A, radius=r, speed=1.0, parallel_agents=A, threads_per_agent=threads_per_agent,
+                            queue_capacity=queue_capacity, steps=500, seed=seed * 1000 + k,
+                            meta={"retarget_p": 0.02}))
+    return out
 
 
 def zigzag() -> Scenario:

@@ -188,8 +188,8 @@ int64_t gmapf_kernel_launches(gmapf_ctx* ctx);
  * time or order their own work against it; null before the start */
 void* gmapf_stream_handle(gmapf_ctx* ctx);
 /* effective search shape after the start: threads per agent, queue
- * capacity, block size, visited mode (1 shared bitmap, 2 global records)
- * and resident lane-group slots */
+ * capacity, block size, visited mode (1 shared bitmap, 2 global records,
+ * 3 global bitmap) and resident request slots */
 gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t* block_threads,
                                 int32_t* visited_mode, int32_t* slots);
 
@@ -209,6 +209,44 @@ gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, 
 /* device time (ms) of the last batch search kernel, measured with CUDA
  * events on the launching stream */
 gmapf_status gmapf_last_search_ms(gmapf_ctx* ctx, float* out_ms);
+
+/* ---- scene batches: several maps stepped as one ----
+ * The reference runs one map per GMAPF instance (a second FillMap* throws
+ * "map is already filled", GMAPF.cu:205-206), so a program with several
+ * scenes creates several instances and steps them in turn.  A scene batch
+ * keeps those instances as they are -- each scene is an ordinary context,
+ * initialised, filled and given its agents through the calls above -- and
+ * steps all of them with one compaction, one persistent search launch and one
+ * mover pass per frame.  Each scene keeps its own Config (radius, speed,
+ * PathFinderParallelAgents, agent count); threads per agent, queue capacity
+ * and heuristic K must be equal across the scenes (they shape the one search
+ * launch).  Results per scene equal those of that scene stepped alone.
+ *
+ * After gmapf_batch_create the scene contexts stay valid for their per-agent
+ * calls (gmapf_set_agent_targ_pos[_bulk], gmapf_get_agent_pos/state,
+ * gmapf_get_agents, gmapf_agent_pos_view, gmapf_debug_get_agents/path,
+ * gmapf_locate_points and the map queries), with the scene's own agent and
+ * triangle ids; stepping, options, statistics and profiling go through the
+ * world context that gmapf_batch_world returns (gmapf_manual_start,
+ * gmapf_async_step, gmapf_wait_step_end, gmapf_last_step_stats, ...).  On
+ * the world, agent and triangle ids are global: scene s's agents start at
+ * agent_base and its triangles at node_base (gmapf_batch_scene_base);
+ * gmapf_set_agent_targ_pos_device on the world takes global agent ids and
+ * locates each target in its agent's scene.  Calls that would change a
+ * scene's map, agent set or options, or step it alone, return GMAPF_E_STATE. */
+typedef struct gmapf_batch gmapf_batch;
+/* Bind n >= 1 scene contexts (initialised, map filled, not started, not in
+ * another batch) into a batch; opt (may be null) holds the world's step
+ * options (mode, device, block size, visited mode, autotune). */
+gmapf_status gmapf_batch_create(gmapf_ctx* const* scenes, int32_t n, const gmapf_options* opt,
+                                gmapf_batch** out);
+/* Free the world; the scene contexts then answer GMAPF_E_STATE to agent calls
+ * and may only be destroyed. */
+gmapf_status gmapf_batch_destroy(gmapf_batch* batch);
+/* the world context (owned by the batch; do not destroy it) */
+gmapf_ctx* gmapf_batch_world(gmapf_batch* batch);
+/* first global agent id and first global triangle id of scene s */
+gmapf_status gmapf_batch_scene_base(gmapf_batch* batch, int32_t scene, int32_t* agent_base, int32_t* node_base);
 
 /* ---- searches without any memory allocation ----
  * No counterpart in the reference.  For callers that may not allocate
