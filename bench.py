@@ -185,6 +185,94 @@ def algorithmic_bytes(st: dict, n_nodes: int) -> float:
             + 4.0 * st["path_nodes"])
 
 
+# ----------------------------------------------------- multi-scene (cfg4) --
+
+def multi_scene(steps: int, warmup: int, n_scenes: int = 64):
+    """64 independent scenes (random sides, obstacles, agent counts and radii),
+    retargets with probability 0.02 per agent per step through each scene's
+    host API.  One scene batch (one compaction, one persistent search launch
+    and one mover pass per frame) against the same scenes as separate
+    contexts stepped in turn -- how the reference runs several maps (one map
+    per GMAPF instance).  Host wall time per frame, retargets included."""
+    import gmapf_b200 as G
+    from gmapf_b200 import scenarios as S
+    scns = S.cfg4(n_scenes, seed=4)
+
+    def scene(scn):
+        g = G.GMAPF()
+        g.Init(G.make_config(scn.agents, scn.radius, scn.speed, scn.agents, scn.threads_per_agent,
+                             scn.queue_capacity, scn.heuristic_k))
+        S.build_map(g, scn)
+        for p in S.free_points(g, scn, scn.agents, np.random.default_rng(scn.seed)):
+            g.AddAgent(p)
+        return g
+
+    # the same retargets for both forms: per step, per scene (ids, points)
+    probe = [scene(scn) for scn in scns]
+    total = warmup + steps
+    plan = []
+    for k in range(total):
+        row = []
+        for scn, g in zip(scns, probe):
+            rng = np.random.default_rng((scn.seed, k))
+            ids = np.arange(scn.agents) if k == 0 else np.nonzero(rng.random(scn.agents) < 0.02)[0]
+            row.append((ids.astype(np.int32), S.free_points(g, scn, len(ids), rng) if len(ids) else None))
+        plan.append(row)
+    for g in probe:
+        g.close()
+    A = sum(s.agents for s in scns)
+    out = {"workload": f"{n_scenes} scenes: sides U[200,2000], U[10,500] rectangles (sides U[10,60]), "
+                       f"U[64,1024] agents of radius U[1,3], retarget p=0.02 per agent per step",
+           "agents": A, "steps": steps, "warmup": warmup}
+
+    def timed(step_fn, scenes):
+        wall = []
+        for k in range(total):
+            t0 = time.perf_counter()
+            for g, (ids, pts) in zip(scenes, plan[k]):
+                if pts is not None:
+                    g.set_targets(ids, pts)
+            step_fn()
+            if k >= warmup:
+                wall.append((time.perf_counter() - t0) * 1e3)
+        return wall
+
+    # one scene batch
+    scenes = [scene(scn) for scn in scns]
+    out["triangles"] = sum(g.node_count for g in scenes)
+    batch = G.SceneBatch(scenes)
+    batch.ManualStart()
+
+    def step_batch():
+        batch.AsyncStep(1.0 / 60.0)
+        batch.WaitStepEnd()
+
+    wb = timed(step_batch, scenes)
+    launches = batch.world.kernel_launches
+    batch.close()
+    for g in scenes:
+        g.close()
+    # separate contexts, stepped in turn
+    seps = [scene(scn) for scn in scns]
+    for g in seps:
+        g.ManualStart()
+
+    def step_sep():
+        for g in seps:
+            g.AsyncStep(1.0 / 60.0)
+            g.WaitStepEnd()
+
+    ws = timed(step_sep, seps)
+    for g in seps:
+        g.close()
+    for name, w in (("batch", wb), ("separate_in_turn", ws)):
+        out[name] = {"ms_per_step": statistics.mean(w), "p50_step_ms": pct(w, 50), "p99_step_ms": pct(w, 99),
+                     "steps_per_s": 1e3 / statistics.mean(w), "agent_steps_per_s": A * 1e3 / statistics.mean(w)}
+    out["batch_over_separate"] = out["batch"]["steps_per_s"] / out["separate_in_turn"]["steps_per_s"]
+    out["batch_kernel_launches"] = launches
+    return out
+
+
 # --------------------------------------------------------------- b200 arm --
 
 def make_scene(cells, seed, T, C, mode, agents, profiler=True, autotune=False):
@@ -358,6 +446,11 @@ def bench_b200(args):
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(g, scn, sets, Tb, Cb, args.cpu_sample, os.cpu_count() or 1)
 
+    # the multi-scene configuration (scene batch against separate contexts)
+    multi = None
+    if rank == 0 and args.multi_scene_steps > 0:
+        multi = multi_scene(args.multi_scene_steps, 3)
+
     # secondary workload: the 64x64-cell maze of the configuration text
     secondary = None
     if args.secondary_cells and args.secondary_cells != args.cells and rank == 0:
@@ -420,6 +513,7 @@ def bench_b200(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "secondary": secondary,
+            "multi_scene": multi,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -480,6 +574,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=160, help="maze cells per side (160: ~100k triangles)")
     ap.add_argument("--secondary-cells", type=int, default=64, help="also report this maze (0: off)")
+    ap.add_argument("--multi-scene-steps", type=int, default=100,
+                    help="frames of the 64-scene configuration, batch vs separate contexts (0: off)")
     ap.add_argument("--agents", type=int, default=16384)
     ap.add_argument("--threads-per-agent", type=int, default=8)
     ap.add_argument("--queue-capacity", type=int, default=32)

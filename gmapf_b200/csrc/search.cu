@@ -43,6 +43,8 @@
 //     stop (plain form).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "internal.h"
 
 namespace gmapf_b200 {
@@ -568,14 +570,38 @@ cudaError_t launch_t(cudaStream_t s, const SearchParams& p, int blocks, int bt, 
     return cudaGetLastError();
 }
 
+// The dynamic shared-memory limit is an attribute of the kernel on a device,
+// shared by every context of the process: it is only ever raised, so a
+// context sized for a small map never lowers the limit under a live context
+// sized for a larger one.
+std::mutex g_smem_attr_mu;
+
+template <int T, int VM>
+int& smem_attr(int device) {
+    static int limit[64] = {};
+    return limit[device & 63];
+}
+
 template <int T, int VM>
 int occupancy_t(int C, int bt, int bm_words) {
     const size_t smem = search_smem_bytes(C, bt, VM == 1 ? bm_words : 0, T);
     if (smem > 227 * 1024) return 0;
-    if (cudaFuncSetAttribute(k_search<T, VM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
         cudaGetLastError();
         return 0;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_smem_attr_mu);
+        int& limit = smem_attr<T, VM>(device);
+        if ((int)smem > limit) {
+            if (cudaFuncSetAttribute(k_search<T, VM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                return 0;
+            }
+            limit = (int)smem;
+        }
     }
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<T, VM>, bt, smem) != cudaSuccess) {

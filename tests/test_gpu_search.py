@@ -160,3 +160,16 @@ def test_disconnected_map_not_found(oracle_mod, vm):
     f, l, p, st = g.search_batch(np.array([0, 0, 2], np.int32), np.array([3, 1, 3], np.int32), 4)
     assert f.tolist() == [0, 1, 1]
     assert l.tolist() == [0, 1, 1]
+
+
+def test_live_contexts_with_different_shapes(oracle_mod):
+    # the kernel's shared-memory limit is shared by every context in the process:
+    # a context started later for a smaller map must not break a larger one
+    big_scn, small_scn = S.cfg3(cells=24), S.cfg1()
+    big = map_world(big_scn, T=8, Cap=32, visited_mode=1)
+    s1, t1 = random_queries(big, big_scn, 300, seed=31)
+    check_batch(oracle_mod, big, s1, t1, 8, 32)
+    small = map_world(small_scn, T=8, Cap=4, visited_mode=1)
+    s2, t2 = random_queries(small, small_scn, 300, seed=32)
+    check_batch(oracle_mod, small, s2, t2, 8, 4)
+    check_batch(oracle_mod, big, s1, t1, 8, 32)
