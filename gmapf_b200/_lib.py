@@ -54,6 +54,19 @@ class Options(C.Structure):
     ]
 
 
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64), ("found", C.c_int64),
+        ("applied", C.c_int64), ("superseded", C.c_int64), ("waiting", C.c_int64), ("in_flight", C.c_int64),
+        ("launches", C.c_int64), ("latency_samples", C.c_int64), ("capacity", C.c_int32), ("slots", C.c_int32),
+        ("latency_p50_ms", C.c_float), ("latency_p99_ms", C.c_float), ("latency_mean_ms", C.c_float),
+        ("latency_max_ms", C.c_float),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class StepStats(C.Structure):
     _fields_ = [
         ("requests", C.c_int64), ("found", C.c_int64), ("expansions", C.c_int64),
@@ -120,6 +133,14 @@ SIGNATURES = {
     "gmapf_search_batch_device": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(StepStats)]),
     "gmapf_last_search_ms": (C.c_int, [P, C.POINTER(C.c_float)]),
+    "gmapf_serve_start": (C.c_int, [P, C.c_int32]),
+    "gmapf_serve_submit": (C.c_int, [P, I32P, V2P, C.c_int32, C.POINTER(C.c_int64)]),
+    "gmapf_serve_poll": (C.c_int, [P]),
+    "gmapf_serve_drain": (C.c_int, [P, C.c_float]),
+    "gmapf_serve_get_stats": (C.c_int, [P, C.POINTER(ServeStats), C.c_int32]),
+    "gmapf_serve_result": (C.c_int, [P, C.c_int32, I32P, I32P, I32P, C.c_int32]),
+    "gmapf_serve_stop": (C.c_int, [P]),
+    "gmapf_clock_ns": (C.c_int64, []),
     "gmapf_batch_create": (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(Options), C.POINTER(P)]),
     "gmapf_batch_destroy": (C.c_int, [P]),
     "gmapf_batch_world": (P, [P]),

@@ -204,6 +204,40 @@ class GMAPF:
         self._check(self._lib.gmapf_set_agent_targ_pos_bulk(self._h, _ptr(ids), p.ctypes.data_as(C.POINTER(V2)),
                                                              len(ids)))
 
+    # -- serving (gmapf_serve_*) ---------------------------------------------
+    def serve_start(self, max_in_flight: int = 0) -> None:
+        self._check(self._lib.gmapf_serve_start(self._h, int(max_in_flight)))
+
+    def serve_submit(self, ids, pos, arrival_ns=None) -> None:
+        ids = _i32(ids)
+        p = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 2)
+        arr = None
+        if arrival_ns is not None:
+            arr = np.ascontiguousarray(arrival_ns, dtype=np.int64)
+            arr = arr.ctypes.data_as(C.POINTER(C.c_int64))
+        self._check(self._lib.gmapf_serve_submit(self._h, _ptr(ids), p.ctypes.data_as(C.POINTER(V2)), len(ids), arr))
+
+    def serve_poll(self) -> None:
+        self._check(self._lib.gmapf_serve_poll(self._h))
+
+    def serve_drain(self, timeout_s: float = 60.0) -> None:
+        self._check(self._lib.gmapf_serve_drain(self._h, float(timeout_s)))
+
+    def serve_stats(self, reset: bool = False) -> dict:
+        st = _lib.ServeStats()
+        self._check(self._lib.gmapf_serve_get_stats(self._h, C.byref(st), 1 if reset else 0))
+        return st.as_dict()
+
+    def serve_result(self, agent: int):
+        """(found, length, path) of the agent's finished query not yet installed by a frame."""
+        f, L = C.c_int32(), C.c_int32()
+        out = np.empty(max(1, self.node_count), np.int32)
+        self._check(self._lib.gmapf_serve_result(self._h, int(agent), C.byref(f), C.byref(L), _ptr(out), len(out)))
+        return f.value, L.value, out[:max(0, min(L.value, len(out)))].copy()
+
+    def serve_stop(self) -> None:
+        self._check(self._lib.gmapf_serve_stop(self._h))
+
     def set_targets_device(self, d_ids: int, d_pos: int, n: int) -> None:
         """Retarget n agents from device-resident ids (int32) and positions
         (float32 pairs); raw device addresses, enqueued before the next step."""
@@ -339,3 +373,8 @@ class SceneBatch:
             self.close()
         except Exception:
             pass
+
+
+def clock_ns() -> int:
+    """The host clock serving arrival times are measured in (steady clock, ns)."""
+    return int(_lib.load().gmapf_clock_ns())

@@ -29,7 +29,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["search.cu", "kernels.cu", "device.cu", "noalloc.cu"]
+CU_SOURCES = ["search.cu", "kernels.cu", "device.cu", "serve.cu", "noalloc.cu"]
 CPP_SOURCES = ["hostmap.cpp", "capi.cpp"]
 CDT_SOURCE = "navmesh_cdt.cpp"
 

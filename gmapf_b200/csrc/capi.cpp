@@ -2,6 +2,7 @@
 // bookkeeping of gmapf::GMAPF (src/GMAPF.cu), with the reference's
 // exceptions turned into status codes and a per-thread error message.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -638,6 +639,116 @@ gmapf_status gmapf_last_search_ms(gmapf_ctx* ctx, float* out_ms) {
     if (!out_ms) return fail(GMAPF_E_INVALID_ARG, "null output");
     *out_ms = ctx->c.last_search_ms;
     return GMAPF_OK;
+}
+
+// ------------------------------------------------------------------ serving --
+
+namespace {
+// the context that serves: a bound scene's world
+gmapf_ctx* serving_ctx(gmapf_ctx* ctx) { return ctx->world ? ctx->world : ctx; }
+}  // namespace
+
+gmapf_status gmapf_serve_start(gmapf_ctx* ctx, int32_t max_in_flight) {
+    NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    if (ctx->world) return scene_only("serve start");
+    Context& c = ctx->c;
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    if (max_in_flight < 0) return fail(GMAPF_E_INVALID_ARG, "max_in_flight must be >= 0");
+    if (c.serve) return fail(GMAPF_E_STATE, "already serving");
+    gmapf_status s = start_if_needed(c);
+    if (s != GMAPF_OK) return s;
+    std::string err;
+    int rc = serve_start(c, max_in_flight, err);
+    if (rc) {
+        serve_free(c);
+        return fail(rc, err);
+    }
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_serve_submit(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* targets, int32_t n,
+                                const int64_t* arrival_ns) {
+    NEED_CTX(ctx);
+    if (ctx->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");
+    gmapf_ctx* w = serving_ctx(ctx);
+    Context& c = w->c;
+    if (!c.serve) return fail(GMAPF_E_STATE, "not serving (gmapf_serve_start)");
+    if (n < 0 || (n > 0 && (!ids || !targets))) return fail(GMAPF_E_INVALID_ARG, "bad arrays");
+    if (n == 0) return GMAPF_OK;
+    std::vector<int> gid;
+    const int* use = ids;
+    if (w != ctx) {  // a bound scene: its own ids, offset into the world
+        gid.resize(n);
+        for (int k = 0; k < n; k++) {
+            if (ids[k] < 0 || ids[k] >= ctx->c.A)
+                return fail(GMAPF_E_INVALID_ARG, "agent id " + std::to_string(ids[k]) + " out of range");
+            gid[k] = ids[k] + ctx->c.agent_base;
+        }
+        use = gid.data();
+    }
+    std::string err;
+    int rc = serve_submit(c, use, targets, n, arrival_ns, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_serve_poll(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    Context& c = serving_ctx(ctx)->c;
+    if (!c.serve) return fail(GMAPF_E_STATE, "not serving (gmapf_serve_start)");
+    std::string err;
+    int rc = serve_poll(c, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_serve_drain(gmapf_ctx* ctx, float timeout_s) {
+    NEED_CTX(ctx);
+    Context& c = serving_ctx(ctx)->c;
+    if (!c.serve) return fail(GMAPF_E_STATE, "not serving (gmapf_serve_start)");
+    std::string err;
+    int rc = serve_drain(c, timeout_s, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_serve_get_stats(gmapf_ctx* ctx, gmapf_serve_stats* out, int32_t reset) {
+    NEED_CTX(ctx);
+    if (!out) return fail(GMAPF_E_INVALID_ARG, "null output");
+    Context& c = serving_ctx(ctx)->c;
+    if (!c.serve) return fail(GMAPF_E_STATE, "not serving (gmapf_serve_start)");
+    serve_stats(c, out, reset != 0);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_serve_result(gmapf_ctx* ctx, int32_t agent, int32_t* found, int32_t* len, int32_t* path,
+                                int32_t cap) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (ctx->world) return scene_only("serve result");
+    if (!c.serve) return fail(GMAPF_E_STATE, "not serving (gmapf_serve_start)");
+    if (agent < 0 || agent >= c.A || !found || !len || (cap > 0 && !path))
+        return fail(GMAPF_E_INVALID_ARG, "bad arguments");
+    std::string err;
+    int rc = serve_result(c, agent, found, len, path, cap, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_serve_stop(gmapf_ctx* ctx) {
+    NEED_CTX(ctx);
+    Context& c = serving_ctx(ctx)->c;
+    if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
+    serve_free(c);
+    return GMAPF_OK;
+}
+
+int64_t gmapf_clock_ns(void) {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
 }
 
 // ------------------------------------------------------------ scene batches --

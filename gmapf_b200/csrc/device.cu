@@ -487,6 +487,7 @@ int device_start(Context& c, std::string& err) {
 
 void device_free(Context& c) {
     Device& d = c.dev;
+    serve_free(c);
     if (d.stream) cudaStreamSynchronize(d.stream);
     if (d.stream2) cudaStreamSynchronize(d.stream2);
     destroy_graph(c);
@@ -524,6 +525,10 @@ int device_async_step(Context& c, float dt, std::string& err) {
         c.launches += 1;
         for (const int4& r : c.dirty_recs) c.dirty_slot[r.x] = -1;
         c.dirty_recs.clear();
+    }
+    if (c.serve) {  // serving: finished queries join this frame
+        int rc = serve_before_frame(c, s, err);
+        if (rc) return rc;
     }
     c.h_step[0] = dt;  // each scene's step is speed * dt, rounded once (AgentsMover.h:63)
     CK(cudaMemcpyAsync(d.counters + 8, c.h_step, sizeof(float), cudaMemcpyHostToDevice, s));
@@ -588,6 +593,7 @@ int device_wait_step(Context& c, std::string& err) {
     Device& d = c.dev;
     CK(cudaSetDevice(d.device));
     CK(cudaStreamSynchronize(d.stream));
+    if (c.serve) serve_after_frame(c);
     const auto t1 = std::chrono::steady_clock::now();
     if (c.A > 0) {
         for (int i = 0; i < c.A; i++) {

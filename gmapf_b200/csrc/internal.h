@@ -71,6 +71,14 @@ struct SearchParams {
     int* ag_path_len;
     unsigned long long* stats;  // ST_COUNT counters
     int* err;
+    // serving ring (ring_cap > 0): request r is req[r % ring_cap]; *req_count_d
+    // is the ring's tail (raised by the host while the kernel runs) and
+    // *work_ctr its head, taken by compare-and-swap so it never passes the tail.
+    // Completion: done[r % ring_cap] = (r + 1) << 1 | found and done_ns[...] =
+    // the device's global timer, both in host-mapped memory, after the results.
+    int ring_cap;
+    unsigned long long* done;
+    unsigned long long* done_ns;
 };
 
 // Per-scene constants of the mover and of point location: one entry for a
@@ -276,6 +284,8 @@ struct Profiler {
     int n = 0, n_search = 0, n_mover = 0;
 };
 
+struct Service;  // serve.cu
+
 struct Context {
     bool inited = false, started = false, step_going = false;
     gmapf_config cfg{};
@@ -324,6 +334,7 @@ struct Context {
     int scene_index = -1, agent_base = 0, node_base = 0;
     bool is_world = false;   // the merged context of a batch
     bool detached = false;   // its batch was destroyed
+    Service* serve = nullptr;  // serving form (after gmapf_serve_start)
     int plain_req_count = 0, plain_mv_count = 0;
 };
 
@@ -342,6 +353,17 @@ int device_autotune(Context& c, std::string& err);
 int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
 int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, int id_base,
                               int id_count, std::string& err);
+
+// serve.cu
+int serve_start(Context& c, int max_in_flight, std::string& err);
+void serve_free(Context& c);
+int serve_submit(Context& c, const int* ids, const gmapf_v2* pos, int n, const int64_t* arrival_ns, std::string& err);
+int serve_poll(Context& c, std::string& err);
+int serve_drain(Context& c, double timeout_s, std::string& err);
+int serve_before_frame(Context& c, cudaStream_t s, std::string& err);
+void serve_after_frame(Context& c);
+void serve_stats(Context& c, gmapf_serve_stats* out, bool reset);
+int serve_result(Context& c, int agent, int* found, int* len, int* path, int cap, std::string& err);
 
 // capi.cpp: message returned by gmapf_last_error() on this thread
 void set_last_error(const std::string& msg);

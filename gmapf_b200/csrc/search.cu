@@ -129,6 +129,31 @@ __device__ __forceinline__ void bm_set(unsigned* bm, int n, int dir) {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Serving ring: take the next request index, never past the tail; -1 when the
+// ring is empty (or, after a bounded number of lost races, to leave the rest
+// to the next launch).
+__device__ __forceinline__ int ring_take(int* head, const int* tail) {
+    for (int it = 0; it < 4096; it++) {
+        const int h = *reinterpret_cast<volatile int*>(head);
+        const int t = *reinterpret_cast<const volatile int*>(tail);
+        if (h >= t) return -1;
+        if (atomicCAS(head, h, h + 1) == h) return h;
+    }
+    return -1;
+}
+
+// Serving ring: publish request r's completion after its results (lane 0,
+// after the warp's writes are ordered by __syncwarp)
+__device__ __forceinline__ void ring_complete(const SearchParams& p, int slot_row, int r, int found) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    __threadfence_system();
+    reinterpret_cast<volatile unsigned long long*>(p.done_ns)[slot_row] = t;
+    __threadfence_system();
+    reinterpret_cast<volatile unsigned long long*>(p.done)[slot_row] =
+        ((unsigned long long)(unsigned)(r + 1) << 1) | (unsigned long long)(found ? 1 : 0);
+}
+
 // per-warp shared-memory regions in 4-byte words, rounded to 16 bytes
 __host__ __device__ __forceinline__ size_t search_queue_words(int C, int T) {
     return ((size_t)kEntryWords * C * T + 3) & ~(size_t)3;
@@ -179,16 +204,22 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         int r, R;
         if (persistent) {
             int v = 0;
-            if (lane == 0) v = atomicAdd(p.work_ctr, 1);
+            if (lane == 0) v = p.ring_cap > 0 ? ring_take(p.work_ctr, p.req_count_d) : atomicAdd(p.work_ctr, 1);
             r = __shfl_sync(kFull, v, 0);
-            R = *p.req_count_d;
+            if (p.ring_cap > 0) {
+                if (r < 0) break;
+                R = r + 1;
+            } else {
+                R = *p.req_count_d;
+            }
         } else {
             if (iter > 0) break;
             r = req_base + slot;
             R = p.req_count_h;
         }
         if (r >= R) break;
-        const int4 rq = p.req[r];
+        // ring entries are rewritten by host copies over time: read past L1
+        const int4 rq = p.ring_cap > 0 ? __ldcg(p.req + (r % p.ring_cap)) : p.req[r];
         const int agent = rq.x, start = rq.y, target = rq.z, orow = rq.w;
         if (start < 0 || start >= n_nodes || target < 0 || target >= n_nodes || start == target) {
             const bool bad = start != target || start < 0 || start >= n_nodes;
@@ -201,6 +232,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                     p.ag_path_len[agent] = 0;
                 }
                 if (!bad) atomicAdd(p.stats + ST_FOUND, 1ull);
+                if (p.done) ring_complete(p, orow, r, bad ? 0 : 1);
             }
             continue;
         }
@@ -555,6 +587,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
             atomicAdd(p.stats + ST_CLAIMS, (unsigned long long)claims);
             atomicAdd(p.stats + ST_PATH_NODES, (unsigned long long)L);
             atomicAdd(p.stats + ST_FOUND, (unsigned long long)found);
+            if (p.done) ring_complete(p, orow, r, found);
         }
     }
 }

@@ -248,6 +248,58 @@ gmapf_ctx* gmapf_batch_world(gmapf_batch* batch);
 /* first global agent id and first global triangle id of scene s */
 gmapf_status gmapf_batch_scene_base(gmapf_batch* batch, int32_t scene, int32_t* agent_base, int32_t* node_base);
 
+/* ---- serving: retargets admitted continuously ----
+ * No counterpart in the reference, where a retarget waits for the next
+ * AsyncStep and that frame's search (src/GMAPF.cu:238-289).  After
+ * gmapf_serve_start, gmapf_serve_submit turns each retarget into a query at
+ * once: its start is the triangle under the agent at submission, it enters a
+ * device ring (capacity set by free device memory; the rest waits on the
+ * host), and one persistent search launch drains the ring while the host
+ * appends to it, so queries that arrive while others run join as warps free
+ * up.  Frames keep running: at each AsyncStep the finished queries' paths are
+ * installed into their agents (unless a newer query of the same agent was
+ * submitted), before the frame's compaction and mover; until then an agent
+ * keeps its previous motion.  A query's result depends only on its start,
+ * target and the map, so it is the same alone and among any other queries.
+ * Latency is measured from the arrival time passed in (host steady clock, see
+ * gmapf_clock_ns; now if null) to the device's completion timestamp.  On a
+ * scene batch call these on the world (global agent ids); on a bound scene,
+ * gmapf_serve_submit takes the scene's own agent ids. */
+typedef struct gmapf_serve_stats {
+    int64_t submitted, admitted, completed, found;
+    int64_t applied;     /* results installed into agents */
+    int64_t superseded;  /* results dropped: a newer query of the same agent came */
+    int64_t waiting;     /* submitted, not yet admitted (ring full) */
+    int64_t in_flight;   /* admitted, not finished */
+    int64_t launches;    /* drain launches */
+    int64_t latency_samples;
+    int32_t capacity;    /* ring entries (queries in flight at most) */
+    int32_t slots;       /* resident search slots of the drain launch */
+    float latency_p50_ms, latency_p99_ms, latency_mean_ms, latency_max_ms;
+} gmapf_serve_stats;
+/* allocate the ring (at most max_in_flight entries, 0: up to 65,536, fewer if
+ * free memory is short) and the serving search state; starts the context */
+gmapf_status gmapf_serve_start(gmapf_ctx* ctx, int32_t max_in_flight);
+/* queue n retargets (agent ids, target positions, arrival times or null) */
+gmapf_status gmapf_serve_submit(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* targets, int32_t n,
+                                const int64_t* arrival_ns);
+/* harvest finished queries, admit waiting ones, launch a drain when needed;
+ * call it often (it never blocks on the GPU) */
+gmapf_status gmapf_serve_poll(gmapf_ctx* ctx);
+/* poll until every submitted query has finished (or timeout_s passes:
+ * GMAPF_E_DEVICE_TIMEOUT) */
+gmapf_status gmapf_serve_drain(gmapf_ctx* ctx, float timeout_s);
+/* counters and latency percentiles since the last reset */
+gmapf_status gmapf_serve_get_stats(gmapf_ctx* ctx, gmapf_serve_stats* out, int32_t reset);
+/* an agent's finished query not yet installed by a frame: found flag, length
+ * and up to cap path triangles (global ids on a world) */
+gmapf_status gmapf_serve_result(gmapf_ctx* ctx, int32_t agent, int32_t* found, int32_t* len, int32_t* path,
+                                int32_t cap);
+/* stop serving and free its memory (pending queries are dropped) */
+gmapf_status gmapf_serve_stop(gmapf_ctx* ctx);
+/* the host clock arrival times are measured in (steady clock, ns) */
+int64_t gmapf_clock_ns(void);
+
 /* ---- searches without any memory allocation ----
  * No counterpart in the reference.  For callers that may not allocate
  * device memory themselves or through the library (an engine that owns every
