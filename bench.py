@@ -273,6 +273,86 @@ def multi_scene(steps: int, warmup: int, n_scenes: int = 64):
     return out
 
 
+# --------------------------------------------------------- serving (cfg5) --
+
+def serving(rates, duration_s: float, n_scenes: int = 8, agents: int = 8192):
+    """Serving loop: n_scenes resident scenes of the 1000x1000, 200-rectangle
+    type (different seeds), `agents` agents each, one scene batch.  Retargets
+    of uniformly chosen agents to uniform free points arrive as a Poisson
+    process at each rate for duration_s; frames (movement and collision
+    avoidance for every agent) run every 1/60 s.  Latency: arrival (the
+    Poisson time) to the query's device completion timestamp."""
+    import gmapf_b200 as G
+    from gmapf_b200 import scenarios as S
+    from gmapf_b200.api import clock_ns
+    scns = [S.cfg2(seed=21 + k) for k in range(n_scenes)]
+    scenes = []
+    for scn in scns:
+        g = G.GMAPF()
+        g.Init(G.make_config(agents, scn.radius, scn.speed, agents, scn.threads_per_agent, scn.queue_capacity,
+                             scn.heuristic_k))
+        S.build_map(g, scn)
+        for p in S.free_points(g, scn, agents, np.random.default_rng(scn.seed)):
+            g.AddAgent(p)
+        scenes.append(g)
+    # targets: a pool of free points per scene
+    pools = [S.free_points(g, scn, 65536, np.random.default_rng(scn.seed + 500)) for g, scn in zip(scenes, scns)]
+    batch = G.SceneBatch(scenes)
+    w = batch.world
+    w.serve_start()
+    A = n_scenes * agents
+    frame_ns = int(1e9 / 60)
+    out = {"workload": f"{n_scenes} resident scenes (1000x1000, 200 rectangles, seeds 21..{20 + n_scenes}), "
+                       f"{agents} agents each ({A} total); Poisson retargets of uniform agents to uniform free "
+                       f"points; frames every 1/60 s", "agents": A, "triangles": w.node_count,
+           "duration_s": duration_s, "rates": []}
+    rng = np.random.default_rng(99)
+    for rate in rates:
+        n = int(rate * duration_s)
+        arr = np.cumsum(rng.exponential(1.0 / rate, n))
+        arr = arr[arr < duration_s]
+        ids = rng.integers(0, A, len(arr)).astype(np.int32)
+        sc = ids // agents
+        pos = np.stack([pools[s][rng.integers(0, 65536)] for s in sc]) if len(ids) else np.zeros((0, 2), np.float32)
+        w.serve_drain()
+        w.serve_stats(reset=True)
+        steps = []
+        t0 = clock_ns()
+        arr_ns = (t0 + arr * 1e9).astype(np.int64)
+        nxt, k = t0, 0
+        end = t0 + int(duration_s * 1e9)
+        while True:
+            now = clock_ns()
+            if now >= end and k >= len(arr_ns):
+                break
+            j = int(np.searchsorted(arr_ns, now, side="right"))
+            if j > k:
+                w.serve_submit(ids[k:j], pos[k:j], arr_ns[k:j])
+                k = j
+            w.serve_poll()
+            if now >= nxt:
+                f0 = clock_ns()
+                w.AsyncStep(1.0 / 60.0)
+                w.serve_poll()
+                w.WaitStepEnd()
+                steps.append((clock_ns() - f0) * 1e-6)
+                nxt += frame_ns
+        w.serve_drain()
+        st = w.serve_stats()
+        out["rates"].append({
+            "offered_qps": rate, "submitted": int(st["submitted"]), "completed": int(st["completed"]),
+            "found": int(st["found"]), "served_qps": st["completed"] / duration_s,
+            "latency_p50_ms": st["latency_p50_ms"], "latency_p99_ms": st["latency_p99_ms"],
+            "latency_mean_ms": st["latency_mean_ms"], "latency_max_ms": st["latency_max_ms"],
+            "batch_launches": int(st["launches"]), "ring_capacity": int(st["capacity"]),
+            "frames": len(steps), "step_p50_ms": pct(steps, 50), "step_p99_ms": pct(steps, 99)})
+    w.serve_stop()
+    batch.close()
+    for g in scenes:
+        g.close()
+    return out
+
+
 # --------------------------------------------------------------- b200 arm --
 
 def make_scene(cells, seed, T, C, mode, agents, profiler=True, autotune=False):
@@ -451,6 +531,11 @@ def bench_b200(args):
     if rank == 0 and args.multi_scene_steps > 0:
         multi = multi_scene(args.multi_scene_steps, 3)
 
+    # the serving configuration (Poisson retargets, frames every 1/60 s)
+    serve = None
+    if rank == 0 and args.serve_seconds > 0:
+        serve = serving([50000, 150000, 500000], args.serve_seconds)
+
     # secondary workload: the 64x64-cell maze of the configuration text
     secondary = None
     if args.secondary_cells and args.secondary_cells != args.cells and rank == 0:
@@ -514,6 +599,7 @@ def bench_b200(args):
             "clocks": clk.summary(),
             "secondary": secondary,
             "multi_scene": multi,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -574,6 +660,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=160, help="maze cells per side (160: ~100k triangles)")
     ap.add_argument("--secondary-cells", type=int, default=64, help="also report this maze (0: off)")
+    ap.add_argument("--serve-seconds", type=float, default=1.0,
+                    help="seconds per arrival rate of the serving configuration (0: off)")
     ap.add_argument("--multi-scene-steps", type=int, default=100,
                     help="frames of the 64-scene configuration, batch vs separate contexts (0: off)")
     ap.add_argument("--agents", type=int, default=16384)

@@ -71,14 +71,15 @@ struct SearchParams {
     int* ag_path_len;
     unsigned long long* stats;  // ST_COUNT counters
     int* err;
-    // serving ring (ring_cap > 0): request r is req[r % ring_cap]; *req_count_d
-    // is the ring's tail (raised by the host while the kernel runs) and
-    // *work_ctr its head, taken by compare-and-swap so it never passes the tail.
-    // Completion: done[r % ring_cap] = (r + 1) << 1 | found and done_ns[...] =
-    // the device's global timer, both in host-mapped memory, after the results.
+    // search state slots [slot_base, slot_base + slots) of rec/epoch/gbm
+    int slot_base;
+    // serving ring (ring_cap > 0): request r of this launch is query
+    // q = ring_base + r, stored at req[q % ring_cap]; its completion word
+    // done[q % ring_cap] = (q + 1) << 1 | found goes to host-mapped memory
+    // after the results
     int ring_cap;
+    int ring_base;
     unsigned long long* done;
-    unsigned long long* done_ns;
 };
 
 // Per-scene constants of the mover and of point location: one entry for a

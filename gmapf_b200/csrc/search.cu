@@ -129,29 +129,12 @@ __device__ __forceinline__ void bm_set(unsigned* bm, int n, int dir) {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// Serving ring: take the next request index, never past the tail; -1 when the
-// ring is empty (or, after a bounded number of lost races, to leave the rest
-// to the next launch).
-__device__ __forceinline__ int ring_take(int* head, const int* tail) {
-    for (int it = 0; it < 4096; it++) {
-        const int h = *reinterpret_cast<volatile int*>(head);
-        const int t = *reinterpret_cast<const volatile int*>(tail);
-        if (h >= t) return -1;
-        if (atomicCAS(head, h, h + 1) == h) return h;
-    }
-    return -1;
-}
-
-// Serving ring: publish request r's completion after its results (lane 0,
+// Serving ring: publish query q's completion after its results (lane 0,
 // after the warp's writes are ordered by __syncwarp)
-__device__ __forceinline__ void ring_complete(const SearchParams& p, int slot_row, int r, int found) {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    __threadfence_system();
-    reinterpret_cast<volatile unsigned long long*>(p.done_ns)[slot_row] = t;
+__device__ __forceinline__ void ring_complete(const SearchParams& p, int slot_row, int q, int found) {
     __threadfence_system();
     reinterpret_cast<volatile unsigned long long*>(p.done)[slot_row] =
-        ((unsigned long long)(unsigned)(r + 1) << 1) | (unsigned long long)(found ? 1 : 0);
+        ((unsigned long long)(unsigned)(q + 1) << 1) | (unsigned long long)(found ? 1 : 0);
 }
 
 // per-warp shared-memory regions in 4-byte words, rounded to 16 bytes
@@ -195,8 +178,8 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                          : nullptr;
 
     if (slot >= p.slots) return;  // whole warps
-    if (VM == 3) bm = p.gbm + (size_t)slot * bm_words;
-    Rec* rec = p.rec + (size_t)slot * n_nodes;
+    if (VM == 3) bm = p.gbm + (size_t)(p.slot_base + slot) * bm_words;
+    Rec* rec = p.rec + (size_t)(p.slot_base + slot) * n_nodes;
     const unsigned lt_mask = (1u << lane) - 1u;
 
     for (int iter = 0;; iter++) {
@@ -204,14 +187,9 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         int r, R;
         if (persistent) {
             int v = 0;
-            if (lane == 0) v = p.ring_cap > 0 ? ring_take(p.work_ctr, p.req_count_d) : atomicAdd(p.work_ctr, 1);
+            if (lane == 0) v = atomicAdd(p.work_ctr, 1);
             r = __shfl_sync(kFull, v, 0);
-            if (p.ring_cap > 0) {
-                if (r < 0) break;
-                R = r + 1;
-            } else {
-                R = *p.req_count_d;
-            }
+            R = *p.req_count_d;
         } else {
             if (iter > 0) break;
             r = req_base + slot;
@@ -219,7 +197,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         }
         if (r >= R) break;
         // ring entries are rewritten by host copies over time: read past L1
-        const int4 rq = p.ring_cap > 0 ? __ldcg(p.req + (r % p.ring_cap)) : p.req[r];
+        const int4 rq = p.ring_cap > 0 ? __ldcg(p.req + ((p.ring_base + r) % p.ring_cap)) : p.req[r];
         const int agent = rq.x, start = rq.y, target = rq.z, orow = rq.w;
         if (start < 0 || start >= n_nodes || target < 0 || target >= n_nodes || start == target) {
             const bool bad = start != target || start < 0 || start >= n_nodes;
@@ -232,7 +210,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
                     p.ag_path_len[agent] = 0;
                 }
                 if (!bad) atomicAdd(p.stats + ST_FOUND, 1ull);
-                if (p.done) ring_complete(p, orow, r, bad ? 0 : 1);
+                if (p.done) ring_complete(p, orow, p.ring_base + r, bad ? 0 : 1);
             }
             continue;
         }
@@ -240,14 +218,14 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
         unsigned ep = 0;
         if (VM == 2) {
             unsigned e = 0;
-            if (lane == 0) e = p.epoch[slot] + 1u;
+            if (lane == 0) e = p.epoch[p.slot_base + slot] + 1u;
             e = __shfl_sync(kFull, e, 0);
             if (e == 0u) {  // 2^32 queries in this slot: wipe its records once
                 for (long long k = lane; k < (long long)n_nodes * 2; k += 32)
                     __stcg(reinterpret_cast<int4*>(rec) + k, make_int4(0, 0, 0, 0));
                 e = 1u;
             }
-            if (lane == 0) p.epoch[slot] = e;
+            if (lane == 0) p.epoch[p.slot_base + slot] = e;
             ep = e;
         } else if (SMEMV) {
             uint4* b4 = reinterpret_cast<uint4*>(bm);
@@ -587,7 +565,7 @@ __global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, 
             atomicAdd(p.stats + ST_CLAIMS, (unsigned long long)claims);
             atomicAdd(p.stats + ST_PATH_NODES, (unsigned long long)L);
             atomicAdd(p.stats + ST_FOUND, (unsigned long long)found);
-            if (p.done) ring_complete(p, orow, r, found);
+            if (p.done) ring_complete(p, orow, p.ring_base + r, found);
         }
     }
 }

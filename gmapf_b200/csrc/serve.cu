@@ -9,12 +9,14 @@
 //     is set by free device memory (one path row per entry plus the search
 //     state); queries beyond the capacity wait on the host until entries are
 //     released;
-//   - one persistent launch of the search kernel drains the ring: a warp that
-//     finishes a query takes the next ring entry, so queries appended while
-//     the launch runs are picked up as warps free up; the host relaunches
-//     when the ring holds work and no launch is in flight;
-//   - each completion writes the device's global timer and a done word into
-//     host-mapped memory; latency = completion - arrival;
+//   - each poll launches the queries admitted since the previous launch as a
+//     micro-batch on one of kStreams streams that is idle; every stream owns
+//     its own range of search slots, so up to kStreams batches run at once
+//     and queries that arrive while others run start without waiting for
+//     them (a persistent launch over its batch: warps take queries as they
+//     free up);
+//   - each completion writes a done word into host-mapped memory after its
+//     results; latency = the host time a poll sees it - the arrival time;
 //   - a finished query's result moves to a per-agent stash (unless a newer
 //     query of the same agent was submitted), which frees its ring entry; at
 //     the next frame boundary a kernel installs the stashed paths into their
@@ -67,12 +69,6 @@ struct ApplyRec {
     float tx, ty;
 };
 
-__global__ void k_globaltimer(unsigned long long* out) {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    *reinterpret_cast<volatile unsigned long long*>(out) = t;
-}
-
 // finished queries -> the per-agent stash (one block per query): {slot, agent}
 __global__ void k_serve_stash(const int2* recs, int n, const int* found, const int* lens, const int* pool,
                               long long stride, int2* stash_fl, int* stash_path) {
@@ -115,25 +111,39 @@ __global__ void k_serve_apply(const ApplyRec* recs, int n, const int2* stash_fl,
 
 }  // namespace
 
+constexpr int kStreams = 8;
+
 struct Service {
     int cap = 0;
-    cudaStream_t stream = nullptr, copy = nullptr, stash_stream = nullptr;
-    cudaEvent_t kdone = nullptr, copied = nullptr, stashed = nullptr, applied_ev = nullptr;
+    // batches
+    cudaStream_t st[kStreams] = {};
+    cudaEvent_t st_done[kStreams] = {};
+    bool st_busy[kStreams] = {};
+    int slots_per_stream = 0;
+    int* d_wc = nullptr;   // per stream: work counter, query count
+    int* h_cnt = nullptr;  // pinned: per stream, the batch's query count
+    int* d_err = nullptr;  // per stream: device-side error bits
+    int* h_err = nullptr;  // pinned copies
+    long long launched = 0;  // queries [launched, tail) admitted, not yet launched
+    // admission copies
+    cudaStream_t copy = nullptr;
+    cudaEvent_t copied = nullptr;
+    bool copy_recorded = false;
+    // stash
+    cudaStream_t stash_stream = nullptr;
+    cudaEvent_t stashed = nullptr, applied_ev = nullptr;
     bool stash_in_flight = false, apply_recorded = false;
     std::vector<int> stashing;  // ring entries freed when `stashed` completes
     int2* d_stash_fl = nullptr;  // per agent: found, length
     int* d_stash_path = nullptr; // per agent: path row
     int2* h_stash = nullptr;
     int2* d_stash_recs = nullptr;
-    bool in_flight = false;
     std::vector<void*> dallocs;
     int4* d_ring = nullptr;
-    int* d_ctr = nullptr;  // [0] head (taken), [1] tail (admitted), [2] error bits
     int *d_found = nullptr, *d_len = nullptr, *d_pool = nullptr;
     long long stride = 0;
-    unsigned long long *h_done = nullptr, *h_done_ns = nullptr;  // host-mapped
-    unsigned long long *d_done = nullptr, *d_done_ns = nullptr;
-    unsigned long long* h_gt = nullptr;                          // host-mapped, calibration
+    unsigned long long* h_done = nullptr;  // host-mapped
+    unsigned long long* d_done = nullptr;
     // the service's own search state
     Rec* rec = nullptr;
     unsigned* epoch = nullptr;
@@ -142,8 +152,6 @@ struct Service {
     unsigned long long* d_stats = nullptr;
     // pinned staging
     int4* h_stage = nullptr;
-    int* h_tail = nullptr;
-    int* h_err = nullptr;
     ApplyRec* h_apply = nullptr;
     ApplyRec* d_apply = nullptr;
     // host bookkeeping
@@ -152,14 +160,13 @@ struct Service {
     std::vector<unsigned char> state;
     std::deque<Waiting> waiting;
     std::vector<unsigned> agent_sub;  // per agent: number of its submissions
-    std::vector<int> install;        // agents with a stashed result to install
+    std::vector<int> install;         // agents with a stashed result to install
     std::vector<unsigned char> to_install;
     std::vector<ApplyRec> target;     // per agent: the stashed result's target
     long long pending = 0;  // admitted, not done
     // statistics
     long long submitted = 0, completed = 0, found = 0, applied = 0, stale = 0, launches = 0;
     std::vector<float> lat_ms;
-    long long gt_offset_ns = 0;  // host steady_clock ns = global timer + offset
 };
 
 namespace {
@@ -222,49 +229,33 @@ int salloc(Service& sv, T** p, size_t count, std::string& err) {
         if (rc_ != GMAPF_OK) return rc_;            \
     } while (0)
 
-// host clock = global timer + offset, from the tightest of a few brackets
-int calibrate(Service& sv, std::string& err) {
-    long long best_w = -1;
-    for (int k = 0; k < 8; k++) {
-        const long long t0 = now_ns();
-        k_globaltimer<<<1, 1, 0, sv.stream>>>(sv.h_gt);
-        SCK(cudaStreamSynchronize(sv.stream));
-        const long long t1 = now_ns();
-        const long long gt = (long long)*reinterpret_cast<volatile unsigned long long*>(sv.h_gt);
-        if (best_w < 0 || t1 - t0 < best_w) {
-            best_w = t1 - t0;
-            sv.gt_offset_ns = (t0 + t1) / 2 - gt;
-        }
-    }
-    return GMAPF_OK;
-}
-
-SearchParams serve_params(Context& c, Service& sv) {
+SearchParams serve_params(Context& c, Service& sv, int k) {
     Device& d = c.dev;
     SearchParams p{};
     p.rows = d.rows;
     p.cen = d.cen;
     p.n = c.map.n;
     p.req = sv.d_ring;
-    p.req_count_d = sv.d_ctr + 1;
+    p.req_count_d = sv.d_wc + 2 * k + 1;
+    p.work_ctr = sv.d_wc + 2 * k;
     p.T = c.T;
     p.C = c.C;
     p.K = c.K;
     p.rec = sv.rec;
     p.epoch = sv.epoch;
-    p.slots = sv.slots;
     p.gbm = sv.gbm;
-    p.work_ctr = sv.d_ctr;
+    p.slot_base = k * sv.slots_per_stream;
+    p.slots = sv.slots_per_stream;
     p.max_rounds = 4 * c.map.n + 64;
     p.paths = sv.d_pool;
     p.path_stride = sv.stride;
     p.out_found = sv.d_found;
     p.out_len = sv.d_len;
     p.stats = sv.d_stats;
-    p.err = sv.d_ctr + 2;
+    p.err = sv.d_err + k;
     p.ring_cap = sv.cap;
+    p.ring_base = (int)sv.launched;
     p.done = sv.d_done;
-    p.done_ns = sv.d_done_ns;
     return p;
 }
 
@@ -278,17 +269,18 @@ int harvest(Context& c, Service& sv, std::string& err) {
         sv.stash_in_flight = false;
     }
     std::vector<int2> fresh;
+    long long now = 0;  // one clock reading for the completions seen by this poll
     for (long long q = sv.released; q < sv.tail; q++) {
         const int slot = (int)(q % sv.cap);
         if (sv.state[slot] != SLOT_ADMITTED) continue;
         const unsigned long long v = reinterpret_cast<volatile unsigned long long*>(sv.h_done)[slot];
         if ((v >> 1) != (unsigned long long)(q + 1)) continue;
-        const unsigned long long t = reinterpret_cast<volatile unsigned long long*>(sv.h_done_ns)[slot];
         const SlotInfo& si = sv.info[slot];
         sv.pending--;
         sv.completed++;
         if (v & 1ull) sv.found++;
-        sv.lat_ms.push_back((float)((double)((long long)t + sv.gt_offset_ns - si.arrival_ns) * 1e-6));
+        if (now == 0) now = now_ns();
+        sv.lat_ms.push_back((float)((double)(now - si.arrival_ns) * 1e-6));
         if (sv.agent_sub[si.agent] == si.sub) {
             fresh.push_back(make_int2(slot, si.agent));
         } else {
@@ -330,10 +322,9 @@ int harvest(Context& c, Service& sv, std::string& err) {
 
 int admit_and_launch(Context& c, Service& sv, std::string& err) {
     // admit waiting queries into free ring entries
-    long long room = sv.cap - (sv.tail - sv.released);
+    const long long room = sv.cap - (sv.tail - sv.released);
     const long long n = std::min<long long>(room, (long long)sv.waiting.size());
     if (n > 0) {
-        SCK(cudaStreamSynchronize(sv.copy));  // staging of the previous admission consumed
         const long long first = sv.tail;
         for (long long k = 0; k < n; k++) {
             const Waiting w = sv.waiting.front();
@@ -349,38 +340,52 @@ int admit_and_launch(Context& c, Service& sv, std::string& err) {
             si.sub = w.sub;
             sv.state[slot] = SLOT_ADMITTED;
         }
-        // the new entries (one or two contiguous ranges), then the tail
+        // the new entries: one or two contiguous ranges of the ring (their
+        // staging entries are not rewritten before the entry is released)
         const int s0 = (int)(first % sv.cap);
         const long long run1 = std::min<long long>(n, sv.cap - s0);
         SCK(cudaMemcpyAsync(sv.d_ring + s0, sv.h_stage + s0, sizeof(int4) * run1, cudaMemcpyHostToDevice, sv.copy));
         if (run1 < n)
             SCK(cudaMemcpyAsync(sv.d_ring, sv.h_stage, sizeof(int4) * (n - run1), cudaMemcpyHostToDevice, sv.copy));
+        SCK(cudaEventRecord(sv.copied, sv.copy));
+        sv.copy_recorded = true;
         sv.tail += n;
         sv.pending += n;
-        *sv.h_tail = (int)sv.tail;
-        SCK(cudaMemcpyAsync(sv.d_ctr + 1, sv.h_tail, sizeof(int), cudaMemcpyHostToDevice, sv.copy));
-        SCK(cudaEventRecord(sv.copied, sv.copy));
     }
-    // one drain launch at a time: a running launch takes new entries itself
-    if (sv.in_flight && cudaEventQuery(sv.kdone) == cudaSuccess) {
-        sv.in_flight = false;
-        if (*sv.h_err != 0) {
-            err = "serving search: device-side check failed (error bits " + std::to_string(*sv.h_err) + ")";
-            *sv.h_err = 0;
+    // finished batches
+    for (int k = 0; k < kStreams; k++) {
+        if (!sv.st_busy[k] || cudaEventQuery(sv.st_done[k]) != cudaSuccess) continue;
+        sv.st_busy[k] = false;
+        if (sv.h_err[k] != 0) {
+            err = "serving search: device-side check failed (error bits " + std::to_string(sv.h_err[k]) + ")";
+            sv.h_err[k] = 0;
             return GMAPF_E_DEVICE;
         }
     }
-    if (!sv.in_flight && sv.pending > 0) {
-        SCK(cudaStreamWaitEvent(sv.stream, sv.copied, 0));
-        SearchParams sp = serve_params(c, sv);
-        const int gpb = c.block_threads / 32;
-        SCK(launch_search(sv.stream, sp, sv.slots / gpb, c.block_threads, true, 0, c.dev.vm, c.dev.bm_words));
-        SCK(cudaMemcpyAsync(sv.h_err, sv.d_ctr + 2, sizeof(int), cudaMemcpyDeviceToHost, sv.stream));
-        SCK(cudaMemsetAsync(sv.d_ctr + 2, 0, sizeof(int), sv.stream));
-        SCK(cudaEventRecord(sv.kdone, sv.stream));
-        sv.in_flight = true;
-        sv.launches++;
-        c.launches++;
+    // the queries admitted since the last launch, as one batch on an idle stream
+    if (sv.launched < sv.tail) {
+        int k = -1;
+        for (int j = 0; j < kStreams && k < 0; j++)
+            if (!sv.st_busy[j]) k = j;
+        if (k >= 0) {
+            const long long cnt = sv.tail - sv.launched;
+            sv.h_cnt[k] = (int)cnt;
+            cudaStream_t st = sv.st[k];
+            if (sv.copy_recorded) SCK(cudaStreamWaitEvent(st, sv.copied, 0));
+            SCK(cudaMemsetAsync(sv.d_wc + 2 * k, 0, sizeof(int), st));
+            SCK(cudaMemcpyAsync(sv.d_wc + 2 * k + 1, sv.h_cnt + k, sizeof(int), cudaMemcpyHostToDevice, st));
+            SearchParams sp = serve_params(c, sv, k);
+            const int gpb = c.block_threads / 32;
+            const long long warps = std::min<long long>(cnt, sv.slots_per_stream);
+            const int blocks = (int)((warps + gpb - 1) / gpb);
+            SCK(launch_search(st, sp, blocks, c.block_threads, true, 0, c.dev.vm, c.dev.bm_words));
+            SCK(cudaMemcpyAsync(sv.h_err + k, sv.d_err + k, sizeof(int), cudaMemcpyDeviceToHost, st));
+            SCK(cudaEventRecord(sv.st_done[k], st));
+            sv.st_busy[k] = true;
+            sv.launched = sv.tail;
+            sv.launches++;
+            c.launches++;
+        }
     }
     return GMAPF_OK;
 }
@@ -394,10 +399,12 @@ int serve_start(Context& c, int max_in_flight, std::string& err) {
     Service* psv = new Service();
     c.serve = psv;
     Service& sv = *psv;
-    SCK(cudaStreamCreateWithFlags(&sv.stream, cudaStreamNonBlocking));
+    for (int k = 0; k < kStreams; k++) {
+        SCK(cudaStreamCreateWithFlags(&sv.st[k], cudaStreamNonBlocking));
+        SCK(cudaEventCreateWithFlags(&sv.st_done[k], cudaEventDisableTiming));
+    }
     SCK(cudaStreamCreateWithFlags(&sv.copy, cudaStreamNonBlocking));
     SCK(cudaStreamCreateWithFlags(&sv.stash_stream, cudaStreamNonBlocking));
-    SCK(cudaEventCreateWithFlags(&sv.kdone, cudaEventDisableTiming));
     SCK(cudaEventCreateWithFlags(&sv.copied, cudaEventDisableTiming));
     SCK(cudaEventCreateWithFlags(&sv.stashed, cudaEventDisableTiming));
     SCK(cudaEventCreateWithFlags(&sv.applied_ev, cudaEventDisableTiming));
@@ -421,12 +428,14 @@ int serve_start(Context& c, int max_in_flight, std::string& err) {
     // block per SM for the frames' own kernels
     const int drain_per_sm = per_sm > 1 ? per_sm - 1 : 1;
     long long slots = std::min<long long>((long long)sms * drain_per_sm * gpb, (long long)(0.25 * freeb / per_slot));
-    slots = (slots / gpb) * gpb;
-    if (slots < gpb) {
-        err = "serving: not enough device memory for one search slot";
+    // split over the streams, whole blocks each
+    const long long per_stream = (slots / kStreams / gpb) * gpb;
+    if (per_stream < gpb) {
+        err = "serving: not enough device memory for the search slots";
         return GMAPF_E_CAPACITY;
     }
-    sv.slots = (int)slots;
+    sv.slots_per_stream = (int)per_stream;
+    sv.slots = (int)(per_stream * kStreams);
     SALLOC(sv.rec, (size_t)sv.slots * n);
     SALLOC(sv.epoch, (size_t)sv.slots);
     if (d.vm == 3) SALLOC(sv.gbm, (size_t)sv.slots * d.bm_words);
@@ -443,7 +452,8 @@ int serve_start(Context& c, int max_in_flight, std::string& err) {
     }
     sv.cap = (int)cap;
     SALLOC(sv.d_ring, (size_t)sv.cap);
-    SALLOC(sv.d_ctr, 4);
+    SALLOC(sv.d_wc, 2 * kStreams);
+    SALLOC(sv.d_err, kStreams);
     SALLOC(sv.d_found, (size_t)sv.cap);
     SALLOC(sv.d_len, (size_t)sv.cap);
     SALLOC(sv.d_pool, (size_t)sv.cap * sv.stride);
@@ -452,39 +462,40 @@ int serve_start(Context& c, int max_in_flight, std::string& err) {
     SALLOC(sv.d_stash_fl, (size_t)std::max(1, c.A));
     SALLOC(sv.d_stash_path, (size_t)std::max(1, c.A) * sv.stride);
     SCK(cudaHostAlloc((void**)&sv.h_done, sizeof(unsigned long long) * sv.cap, cudaHostAllocMapped));
-    SCK(cudaHostAlloc((void**)&sv.h_done_ns, sizeof(unsigned long long) * sv.cap, cudaHostAllocMapped));
-    SCK(cudaHostAlloc((void**)&sv.h_gt, sizeof(unsigned long long), cudaHostAllocMapped));
     std::memset(sv.h_done, 0, sizeof(unsigned long long) * sv.cap);
-    std::memset(sv.h_done_ns, 0, sizeof(unsigned long long) * sv.cap);
     SCK(cudaHostGetDevicePointer((void**)&sv.d_done, sv.h_done, 0));
-    SCK(cudaHostGetDevicePointer((void**)&sv.d_done_ns, sv.h_done_ns, 0));
     SCK(cudaMallocHost((void**)&sv.h_stage, sizeof(int4) * sv.cap));
-    SCK(cudaMallocHost((void**)&sv.h_tail, sizeof(int)));
-    SCK(cudaMallocHost((void**)&sv.h_err, sizeof(int)));
+    SCK(cudaMallocHost((void**)&sv.h_cnt, sizeof(int) * kStreams));
+    SCK(cudaMallocHost((void**)&sv.h_err, sizeof(int) * kStreams));
     SCK(cudaMallocHost((void**)&sv.h_apply, sizeof(ApplyRec) * std::max(1, c.A)));
     SCK(cudaMallocHost((void**)&sv.h_stash, sizeof(int2) * sv.cap));
-    *sv.h_err = 0;
+    std::memset(sv.h_err, 0, sizeof(int) * kStreams);
     sv.info.assign(sv.cap, SlotInfo{});
     sv.state.assign(sv.cap, SLOT_FREE);
     sv.agent_sub.assign(std::max(1, c.A), 0u);
     sv.to_install.assign(std::max(1, c.A), 0);
     sv.target.assign(std::max(1, c.A), ApplyRec{});
-    return calibrate(sv, err);
+    return GMAPF_OK;
 }
 
 void serve_free(Context& c) {
     if (!c.serve) return;
     Service& sv = *c.serve;
-    if (sv.stream) cudaStreamSynchronize(sv.stream);
+    for (int k = 0; k < kStreams; k++)
+        if (sv.st[k]) cudaStreamSynchronize(sv.st[k]);
     if (sv.copy) cudaStreamSynchronize(sv.copy);
     if (sv.stash_stream) cudaStreamSynchronize(sv.stash_stream);
     for (void* p : sv.dallocs) cudaFree(p);
-    void* hp[] = {sv.h_done, sv.h_done_ns, sv.h_gt, sv.h_stage, sv.h_tail, sv.h_err, sv.h_apply, sv.h_stash};
+    void* hp[] = {sv.h_done, sv.h_stage, sv.h_cnt, sv.h_err, sv.h_apply, sv.h_stash};
     for (void* p : hp)
         if (p) cudaFreeHost(p);
-    for (cudaEvent_t e : {sv.kdone, sv.copied, sv.stashed, sv.applied_ev})
+    for (int k = 0; k < kStreams; k++) {
+        if (sv.st_done[k]) cudaEventDestroy(sv.st_done[k]);
+        if (sv.st[k]) cudaStreamDestroy(sv.st[k]);
+    }
+    for (cudaEvent_t e : {sv.copied, sv.stashed, sv.applied_ev})
         if (e) cudaEventDestroy(e);
-    for (cudaStream_t st : {sv.stream, sv.copy, sv.stash_stream})
+    for (cudaStream_t st : {sv.copy, sv.stash_stream})
         if (st) cudaStreamDestroy(st);
     delete c.serve;
     c.serve = nullptr;

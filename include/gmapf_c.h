@@ -254,15 +254,15 @@ gmapf_status gmapf_batch_scene_base(gmapf_batch* batch, int32_t scene, int32_t* 
  * gmapf_serve_start, gmapf_serve_submit turns each retarget into a query at
  * once: its start is the triangle under the agent at submission, it enters a
  * device ring (capacity set by free device memory; the rest waits on the
- * host), and one persistent search launch drains the ring while the host
- * appends to it, so queries that arrive while others run join as warps free
- * up.  Frames keep running: at each AsyncStep the finished queries' paths are
+ * host), and each poll launches the newly admitted queries as a batch on one
+ * of several streams, each with its own search slots, so queries that arrive
+ * while others run start without waiting for them.  Frames keep running: at each AsyncStep the finished queries' paths are
  * installed into their agents (unless a newer query of the same agent was
  * submitted), before the frame's compaction and mover; until then an agent
  * keeps its previous motion.  A query's result depends only on its start,
  * target and the map, so it is the same alone and among any other queries.
  * Latency is measured from the arrival time passed in (host steady clock, see
- * gmapf_clock_ns; now if null) to the device's completion timestamp.  On a
+ * gmapf_clock_ns; now if null) to the poll that sees the query finished.  On a
  * scene batch call these on the world (global agent ids); on a bound scene,
  * gmapf_serve_submit takes the scene's own agent ids. */
 typedef struct gmapf_serve_stats {
@@ -271,10 +271,10 @@ typedef struct gmapf_serve_stats {
     int64_t superseded;  /* results dropped: a newer query of the same agent came */
     int64_t waiting;     /* submitted, not yet admitted (ring full) */
     int64_t in_flight;   /* admitted, not finished */
-    int64_t launches;    /* drain launches */
+    int64_t launches;    /* batch launches */
     int64_t latency_samples;
     int32_t capacity;    /* ring entries (queries in flight at most) */
-    int32_t slots;       /* resident search slots of the drain launch */
+    int32_t slots;       /* search slots over all serving streams */
     float latency_p50_ms, latency_p99_ms, latency_mean_ms, latency_max_ms;
 } gmapf_serve_stats;
 /* allocate the ring (at most max_in_flight entries, 0: up to 65,536, fewer if
@@ -283,8 +283,8 @@ gmapf_status gmapf_serve_start(gmapf_ctx* ctx, int32_t max_in_flight);
 /* queue n retargets (agent ids, target positions, arrival times or null) */
 gmapf_status gmapf_serve_submit(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* targets, int32_t n,
                                 const int64_t* arrival_ns);
-/* harvest finished queries, admit waiting ones, launch a drain when needed;
- * call it often (it never blocks on the GPU) */
+/* harvest finished queries, admit waiting ones and launch them; call it
+ * often: latency is counted to the poll that sees a query finished */
 gmapf_status gmapf_serve_poll(gmapf_ctx* ctx);
 /* poll until every submitted query has finished (or timeout_s passes:
  * GMAPF_E_DEVICE_TIMEOUT) */
