@@ -37,7 +37,7 @@ namespace gmapf_b200 {
 
 namespace {
 
-// device counters: [8] holds the frame's speed*dt as a float
+// device counters: [8] holds the frame's dt as a float
 enum Counter { CT_REQ = 0, CT_MOVE = 1, CT_WORK = 2, CT_ERR = 3, CT_ERR_TARGETS = 4, CT_COUNT = 16 };
 
 template <class T>
@@ -925,6 +925,19 @@ int device_autotune(Context& c, std::string& err) {
             if ((double)t.found >= (double)best_found * 0.999 && (!pick || t.ms < pick->ms)) pick = &t;
         return pick;
     };
+    // stage 1b: the four fastest eligible shapes timed again (four more runs
+    // each), so that shapes within the timing noise are told apart fairly
+    {
+        long long best_found = 0;
+        for (const Trial& t : trials) best_found = std::max(best_found, t.found);
+        std::vector<Trial> top;
+        for (const Trial& t : trials)
+            if ((double)t.found >= (double)best_found * 0.999) top.push_back(t);
+        std::sort(top.begin(), top.end(), [](const Trial& a, const Trial& b) { return a.ms < b.ms; });
+        if (top.size() > 4) top.resize(4);
+        for (int rep = 0; rep < 2; rep++)
+            for (const Trial& t : top) trial(t.T, t.C, t.vm, 0);
+    }
     // stage 2: block size for the chosen shape
     if (const Trial* p1 = choose(); p1 && c.opt.block_threads == 0) {
         const Trial t1 = *p1;
