@@ -147,6 +147,19 @@ class GMAPF:
         arr = np.ascontiguousarray(nodes, dtype=NODE_DTYPE)
         self._check(self._lib.gmapf_fill_map_manually(self._h, arr.ctypes.data_as(C.POINTER(Node)), len(arr)))
 
+    # -- navmesh files -----------------------------------------------------
+    def map_save(self, path) -> None:
+        self._check(self._lib.gmapf_map_save(self._h, str(path).encode()))
+
+    def map_load(self, path) -> None:
+        self._check(self._lib.gmapf_map_load(self._h, str(path).encode()))
+
+    def FillMapEndCached(self, path) -> bool:
+        """FillMapEnd through a cache file; True when the cached navmesh was used."""
+        hit = C.c_int32()
+        self._check(self._lib.gmapf_fill_map_end_cached(self._h, str(path).encode(), C.byref(hit)))
+        return bool(hit.value)
+
     def AsyncStep(self, delta_time: float) -> None:
         self._check(self._lib.gmapf_async_step(self._h, float(delta_time)))
 

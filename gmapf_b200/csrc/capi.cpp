@@ -78,6 +78,8 @@ int add_dirty(Context& c, int id, int node, float x, float y) {
     return GMAPF_OK;
 }
 
+uint64_t cdt_input_hash(const Context& c);  // navmesh files, below
+
 gmapf_status start_if_needed(Context& c) {
     if (c.started) return GMAPF_OK;
     if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
@@ -231,7 +233,9 @@ gmapf_status gmapf_fill_map_end(gmapf_ctx* ctx) {
     std::string err;
     int rc = build_navmesh_cdt(c.cdt_v, c.cdt_e, nodes, err);
     if (rc) return fail(rc, err);
-    return gmapf_fill_map_manually(ctx, nodes.data(), (int32_t)nodes.size());
+    gmapf_status s = gmapf_fill_map_manually(ctx, nodes.data(), (int32_t)nodes.size());
+    if (s == GMAPF_OK) c.map_input_hash = cdt_input_hash(c);
+    return s;
 }
 
 gmapf_status gmapf_fill_map_manually(gmapf_ctx* ctx, const gmapf_node* nodes, int32_t count) {
@@ -251,6 +255,140 @@ gmapf_status gmapf_fill_map_manually(gmapf_ctx* ctx, const gmapf_node* nodes, in
         }
     build_host_map(nodes, count, c.map);
     c.map_filled = true;
+    return GMAPF_OK;
+}
+
+// ------------------------------------------------------------ navmesh files --
+
+}  // extern "C"
+
+namespace {
+
+const char kMapMagic[8] = {'G', 'M', 'A', 'P', 'F', 'N', 'M', '1'};
+
+struct MapFileHeader {
+    char magic[8];
+    uint32_t version;
+    int32_t count;
+    uint64_t input_hash;  // FNV-1a of the FillMapStart/FillMapObstacle input (0: none)
+    uint64_t checksum;    // FNV-1a of the node records
+};
+
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < bytes; i++) {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+uint64_t cdt_input_hash(const Context& c) {
+    uint64_t h = fnv1a(c.cdt_v.data(), sizeof(float) * c.cdt_v.size());
+    h = fnv1a(c.cdt_e.data(), sizeof(unsigned) * c.cdt_e.size(), h);
+    return h ? h : 1;
+}
+
+int write_map(const std::vector<gmapf_node>& nodes, uint64_t input_hash, const char* path, std::string& err) {
+    MapFileHeader hd{};
+    std::memcpy(hd.magic, kMapMagic, 8);
+    hd.version = 1;
+    hd.count = (int32_t)nodes.size();
+    hd.input_hash = input_hash;
+    hd.checksum = fnv1a(nodes.data(), sizeof(gmapf_node) * nodes.size());
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        err = std::string("cannot open ") + path + " for writing";
+        return GMAPF_E_INVALID_ARG;
+    }
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1;
+    if (ok && !nodes.empty()) ok = std::fwrite(nodes.data(), sizeof(gmapf_node), nodes.size(), f) == nodes.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) {
+        err = std::string("cannot write ") + path;
+        return GMAPF_E_INVALID_ARG;
+    }
+    return GMAPF_OK;
+}
+
+int read_map(const char* path, std::vector<gmapf_node>& nodes, uint64_t& input_hash, std::string& err) {
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) {
+        err = std::string("cannot open ") + path;
+        return GMAPF_E_INVALID_ARG;
+    }
+    MapFileHeader hd{};
+    bool ok = std::fread(&hd, sizeof(hd), 1, f) == 1 && std::memcmp(hd.magic, kMapMagic, 8) == 0 && hd.version == 1 &&
+              hd.count >= 0 && hd.count <= (1 << 27);
+    if (ok) {
+        nodes.resize(hd.count);
+        ok = hd.count == 0 || std::fread(nodes.data(), sizeof(gmapf_node), hd.count, f) == (size_t)hd.count;
+        char extra;
+        ok = ok && std::fread(&extra, 1, 1, f) == 0;  // nothing after the records
+    }
+    std::fclose(f);
+    if (ok) ok = fnv1a(nodes.data(), sizeof(gmapf_node) * nodes.size()) == hd.checksum;
+    if (!ok) {
+        err = std::string(path) + " is not an intact navmesh file";
+        return GMAPF_E_INVALID_ARG;
+    }
+    input_hash = hd.input_hash;
+    return GMAPF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gmapf_status gmapf_map_save(gmapf_ctx* ctx, const char* path) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!path) return fail(GMAPF_E_INVALID_ARG, "null path");
+    if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
+    std::string err;
+    int rc = write_map(c.map.nodes, c.map_input_hash, path, err);
+    if (rc) return fail(rc, err);
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_map_load(gmapf_ctx* ctx, const char* path) {
+    NEED_CTX(ctx);
+    if (!path) return fail(GMAPF_E_INVALID_ARG, "null path");
+    std::vector<gmapf_node> nodes;
+    uint64_t h = 0;
+    std::string err;
+    int rc = read_map(path, nodes, h, err);
+    if (rc) return fail(rc, err);
+    gmapf_status s = gmapf_fill_map_manually(ctx, nodes.data(), (int32_t)nodes.size());
+    if (s == GMAPF_OK) ctx->c.map_input_hash = h;
+    return s;
+}
+
+gmapf_status gmapf_fill_map_end_cached(gmapf_ctx* ctx, const char* path, int32_t* hit) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (!path) return fail(GMAPF_E_INVALID_ARG, "null path");
+    if (hit) *hit = 0;
+    if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
+    if (c.started) return fail(GMAPF_E_STATE, "cannot modify map after start");
+    if (c.map_filled) return fail(GMAPF_E_STATE, "map is already filled");
+    const uint64_t want = cdt_input_hash(c);
+    {
+        std::vector<gmapf_node> nodes;
+        uint64_t h = 0;
+        std::string err;
+        if (read_map(path, nodes, h, err) == GMAPF_OK && h == want &&
+            gmapf_fill_map_manually(ctx, nodes.data(), (int32_t)nodes.size()) == GMAPF_OK) {
+            c.map_input_hash = want;
+            if (hit) *hit = 1;
+            return GMAPF_OK;
+        }
+    }
+    gmapf_status s = gmapf_fill_map_end(ctx);
+    if (s != GMAPF_OK) return s;
+    std::string err;
+    int rc = write_map(c.map.nodes, want, path, err);
+    if (rc) return fail(rc, err);
     return GMAPF_OK;
 }
 

@@ -295,6 +295,7 @@ struct Context {
     std::vector<float> cdt_v;
     std::vector<unsigned> cdt_e;
     bool map_filled = false;
+    uint64_t map_input_hash = 0;  // hash of the CDT input the map was built from (0: given as nodes)
     HostMap map;
     // agents: host mirror (capacity reserved at Init, so pointers stay valid)
     int A = 0;
