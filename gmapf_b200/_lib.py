@@ -50,7 +50,8 @@ class Options(C.Structure):
         ("search_mem_budget", C.c_int64),
         ("order_by_estimate", C.c_int32),
         ("visited_mode", C.c_int32),
-        ("_reserved", C.c_int32 * 4),
+        ("path_smoothing", C.c_int32),
+        ("_reserved", C.c_int32 * 3),
     ]
 
 

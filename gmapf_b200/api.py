@@ -60,8 +60,10 @@ def make_config(agents_max: int, radius: float, speed: float, parallel_agents: i
 
 
 def make_options(mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0, autotune: bool = False,
-                 search_mem_budget: int = 0, order_by_estimate: bool = True, visited_mode: int = 0) -> Options:
+                 search_mem_budget: int = 0, order_by_estimate: bool = True, visited_mode: int = 0,
+                 path_smoothing: bool = False) -> Options:
     o = Options()
+    o.path_smoothing = 1 if path_smoothing else 0
     o.device = device
     o.mode = mode
     o.block_threads = block_threads

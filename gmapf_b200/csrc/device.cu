@@ -186,6 +186,7 @@ MoverParams mover_params(Context& c) {
     p.cell_items = d.cell_items;
     p.tri = d.tri;
     p.cen = d.cen;
+    p.waypoints = d.waypoints;
     p.n = c.map.n;
     p.stats = d.stats;
     p.err = d.counters + CT_ERR;
@@ -312,6 +313,7 @@ int enqueue_frame(Context& c, bool timing, std::string& err) {
     MoverParams mp = mover_params(c);
     if (c.A > 0) {
         CK(cudaMemsetAsync(d.cell_cnt, 0, sizeof(int) * (d.cells + 1), s2));
+        launch_funnel(s2, mp);  // path smoothing only
         launch_move_bin(s2, mp);
         launch_cell_scan(s2, mp);
         launch_scatter(s2, mp);
@@ -350,7 +352,9 @@ int capture_graph(Context& c, std::string& err) {
     return GMAPF_OK;
 }
 
-int kernels_per_frame(Context& c) { return 2 + (c.dev.lm ? 1 : 0) + (c.A > 0 ? 4 : 0); }
+int kernels_per_frame(Context& c) {
+    return 2 + (c.dev.lm ? 1 : 0) + (c.A > 0 ? 4 + (c.dev.waypoints ? 1 : 0) : 0);
+}
 
 }  // namespace
 
@@ -411,6 +415,16 @@ int device_start(Context& c, std::string& err) {
         }
     }
     DALLOC(d.paths, (size_t)std::max(1, A) * d.path_stride);
+    if (c.opt.path_smoothing) {
+        size_t freeb = 0, totalb = 0;
+        CK(cudaMemGetInfo(&freeb, &totalb));
+        const double need = (double)std::max(1, A) * d.path_stride * sizeof(float2);
+        if (need > 0.45 * (double)freeb) {
+            err = "path smoothing: steering points (agents x triangles x 8 bytes) exceed the device memory budget";
+            return GMAPF_E_CAPACITY;
+        }
+        DALLOC(d.waypoints, (size_t)std::max(1, A) * d.path_stride);
+    }
     DALLOC(d.req, std::max(1, c.cfg.PathFinderParallelAgents));
     DALLOC(d.counters, CT_COUNT);
     if (c.opt.order_by_estimate && c.opt.mode == GMAPF_MODE_BATCHED && n > 0 && nsc == 1) {
@@ -571,11 +585,12 @@ int device_async_step(Context& c, float dt, std::string& err) {
         if (M > 0) {
             MoverParams mp = mover_params(c);
             CK(cudaMemsetAsync(d.cell_cnt, 0, sizeof(int) * (d.cells + 1), s));
+            launch_funnel(s, mp);  // path smoothing only
             launch_move_bin(s, mp);
             launch_cell_scan(s, mp);
             launch_scatter(s, mp);
             launch_collide_progress(s, mp);
-            c.launches += 4;
+            c.launches += 4 + (d.waypoints ? 1 : 0);
         }
         if (timing) CK(cudaEventRecord(d.ev[3], s));
         if (c.A > 0) {

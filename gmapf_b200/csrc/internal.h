@@ -123,6 +123,7 @@ struct MoverParams {
     // map
     const float2* tri; // 3 vertices per triangle, global ids
     const float2* cen;
+    float2* waypoints; // path smoothing: per agent, per path step, the steering point (null: centroids)
     int n;
     unsigned long long* stats;
     int* err;
@@ -154,6 +155,8 @@ void launch_move_bin(cudaStream_t s, const MoverParams& p);
 void launch_cell_scan(cudaStream_t s, const MoverParams& p);
 void launch_scatter(cudaStream_t s, const MoverParams& p);
 void launch_collide_progress(cudaStream_t s, const MoverParams& p);
+// path smoothing: funnel corners of the paths that start this frame
+void launch_funnel(cudaStream_t s, const MoverParams& p);
 void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets, int n, int nodes,
                           int4* req, int* req_count, int* work_ctr, int* err);
 // search.cu
@@ -257,6 +260,7 @@ struct Device {
     ScenePar* scene_par = nullptr;
     int* agent_scene = nullptr;
     int *scene_abase = nullptr, *scene_P = nullptr, *scene_first = nullptr;
+    float2* waypoints = nullptr;  // path smoothing (A x path_stride)
     // batch API scratch
     int4* breq = nullptr;
     int breq_cap = 0;

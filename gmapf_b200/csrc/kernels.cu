@@ -422,7 +422,7 @@ __global__ void k_collide_progress(MoverParams p) {
         const int nd = path[0];
         p.step_idx[i] = 0;
         p.step_node[i] = nd;
-        p.step_pos[i] = p.cen[nd];
+        p.step_pos[i] = p.waypoints ? p.waypoints[(long long)i * p.path_stride] : p.cen[nd];
         return;
     }
     const int sn = p.step_node[i];
@@ -430,10 +430,26 @@ __global__ void k_collide_progress(MoverParams p) {
         atomicOr(p.err, ERR_BOUNDS);
         return;
     }
-    if (!point_in_tri(np.x, np.y, p.tri[3 * sn], p.tri[3 * sn + 1], p.tri[3 * sn + 2]))
-        return;
-    p.cur_node[i] = sn;
-    if (si < L) si += 1;
+    const bool inside = point_in_tri(np.x, np.y, p.tri[3 * sn], p.tri[3 * sn + 1], p.tri[3 * sn + 2]);
+    bool at_point = false;  // path smoothing: the steering point reached
+    if (p.waypoints && !inside) {
+        const float2 s = p.step_pos[i];
+        const float dx = GM_FSUB(s.x, np.x), dy = GM_FSUB(s.y, np.y);
+        at_point = GM_FSQRT(GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy))) <= sc.arrive;
+    }
+    if (!inside && !at_point) return;
+    if (inside) {
+        p.cur_node[i] = sn;
+        if (si < L) si += 1;
+    } else {
+        // a straight run to a funnel corner may cross thin corridor triangles
+        // between two frames: skip every step that steers to the same point
+        const float2 s = p.step_pos[i];
+        const float2* wp = p.waypoints + (long long)i * p.path_stride;
+        int cur = p.cur_node[i];
+        while (si < L && wp[si].x == s.x && wp[si].y == s.y) cur = path[si++];
+        p.cur_node[i] = cur;
+    }
     p.step_idx[i] = si;
     if (si == L) {
         const float2 t = p.targ_pos[i];
@@ -446,7 +462,126 @@ __global__ void k_collide_progress(MoverParams p) {
     } else {
         const int nd = path[si];
         p.step_node[i] = nd;
-        p.step_pos[i] = p.cen[nd];
+        p.step_pos[i] = p.waypoints ? p.waypoints[(long long)i * p.path_stride + si] : p.cen[nd];
+    }
+}
+
+// ---- path smoothing (opt-in): the simple stupid funnel (M. Mononen, 2010)
+// over the corridor of a path.  Portal 0 is the agent's position, portal k
+// (1..L) the edge shared by triangles k-1 and k of the corridor (triangle 0 =
+// the start triangle, triangle k = path[k-1]), portal L+1 the target
+// position.  Step k of the path (heading into path[k]) steers to the first
+// funnel corner at a portal index >= k+1.
+
+// twice the signed area of (a, b, c): > 0 when c lies left of a -> b
+__device__ __forceinline__ float area2(float2 a, float2 b, float2 c) {
+    const float bx = GM_FSUB(b.x, a.x), by = GM_FSUB(b.y, a.y);
+    const float cx = GM_FSUB(c.x, a.x), cy = GM_FSUB(c.y, a.y);
+    return GM_FSUB(GM_FMUL(bx, cy), GM_FMUL(cx, by));
+}
+
+__device__ __forceinline__ bool veq(float2 a, float2 b) { return a.x == b.x && a.y == b.y; }
+
+// portal k as (left, right) seen travelling from triangle k-1 to triangle k;
+// triangles that share no edge give their centroid as a point portal
+__device__ void corridor_portal(const MoverParams& p, const int* path, int start_tri, int L, float2 sp, float2 ep,
+                                int k, float2& left, float2& right) {
+    if (k <= 0) {
+        left = right = sp;
+        return;
+    }
+    if (k > L) {
+        left = right = ep;
+        return;
+    }
+    const int u = k == 1 ? start_tri : path[k - 2];
+    const int v = path[k - 1];
+    if (u < 0 || u >= p.n || v < 0 || v >= p.n) {
+        left = right = ep;
+        return;
+    }
+    const float2* A = p.tri + 3 * (size_t)u;
+    const float2* B = p.tri + 3 * (size_t)v;
+    float2 s0 = make_float2(0.f, 0.f), s1 = s0;
+    int cnt = 0;
+    for (int a = 0; a < 3; a++) {
+        const float2 va = A[a];
+        if (veq(va, B[0]) || veq(va, B[1]) || veq(va, B[2])) {
+            if (cnt == 0) s0 = va;
+            if (cnt == 1) s1 = va;
+            cnt++;
+        }
+    }
+    if (cnt < 2) {
+        left = right = p.cen[v];
+        return;
+    }
+    if (area2(p.cen[u], p.cen[v], s0) > 0.f) {
+        left = s0;
+        right = s1;
+    } else {
+        left = s1;
+        right = s0;
+    }
+}
+
+// one thread per agent whose path starts this frame (in Move at the frame's
+// start, step index -1): fills its path row of steering points
+__global__ void k_funnel(MoverParams p) {
+    if (*p.mv_count == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.A) return;
+    if (!p.in_move[i] || p.step_idx[i] != -1) return;
+    const int L = p.path_len[i];
+    if (L < 1 || L > p.path_stride) return;
+    const int* path = p.paths + (long long)i * p.path_stride;
+    float2* wp = p.waypoints + (long long)i * p.path_stride;
+    const float2 sp = p.pos[i], ep = p.targ_pos[i];
+    const int st = p.cur_node[i];
+    float2 apex = sp, fl = sp, fr = sp;
+    int apex_i = 0, left_i = 0, right_i = 0, filled = 0;
+    const int max_iter = 4 * (L + 2) + 16;  // every restart moves the apex forward
+    int iter = 0;
+    bool capped = false;
+    for (int k = 1; k <= L + 1; k++) {
+        if (++iter > max_iter) {
+            capped = true;
+            break;
+        }
+        float2 l, r;
+        corridor_portal(p, path, st, L, sp, ep, k, l, r);
+        if (area2(apex, fr, r) >= 0.f) {  // right edge moves inward
+            if (veq(apex, fr) || area2(apex, fl, r) < 0.f) {
+                fr = r;
+                right_i = k;
+            } else {  // crosses the left edge: its end is a corner
+                for (const int upto = min(left_i, L); filled < upto; filled++) wp[filled] = fl;
+                apex = fl;
+                apex_i = left_i;
+                fr = fl = apex;
+                right_i = left_i = apex_i;
+                k = apex_i;
+                continue;
+            }
+        }
+        if (area2(apex, fl, l) <= 0.f) {  // left edge moves inward
+            if (veq(apex, fl) || area2(apex, fr, l) > 0.f) {
+                fl = l;
+                left_i = k;
+            } else {  // crosses the right edge
+                for (const int upto = min(right_i, L); filled < upto; filled++) wp[filled] = fr;
+                apex = fr;
+                apex_i = right_i;
+                fl = fr = apex;
+                left_i = right_i = apex_i;
+                k = apex_i;
+                continue;
+            }
+        }
+    }
+    for (; filled < L; filled++) {
+        const int nd = path[filled];
+        wp[filled] = (capped && nd >= 0 && nd < p.n) ? p.cen[nd] : ep;
     }
 }
 
@@ -494,6 +629,11 @@ void launch_cell_scan(cudaStream_t s, const MoverParams& p) { k_cell_scan<<<1, 1
 
 void launch_scatter(cudaStream_t s, const MoverParams& p) {
     k_scatter<<<blocks_for(p.A, 256), 256, 0, s>>>(p);
+}
+
+void launch_funnel(cudaStream_t s, const MoverParams& p) {
+    if (p.A <= 0 || !p.waypoints) return;
+    k_funnel<<<blocks_for(p.A, 128), 128, 0, s>>>(p);
 }
 
 void launch_collide_progress(cudaStream_t s, const MoverParams& p) {

@@ -90,7 +90,11 @@ typedef struct gmapf_options {
                                   landmark hop-distance estimate first; results do not depend on it */
     int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records,
                                   3 global bitmap per slot (L2-resident for maps up to a few 100k triangles) */
-    int32_t _reserved[4];
+    int32_t path_smoothing;    /* 1: agents steer through the corridor's funnel corners (portal edges)
+                                  instead of triangle centroids; the triangle paths and the per-triangle
+                                  progress stay the reference's.  Off (0) by default: on, agents take
+                                  different routes from the reference's (AgentsMover.h:148,174) */
+    int32_t _reserved[3];
 } gmapf_options;
 
 typedef struct gmapf_step_stats {

@@ -348,6 +348,7 @@ struct Agent {
     std::vector<int> path;
     int step_idx, step_node;
     float sx, sy;
+    std::vector<float> wp;  /* path smoothing: steering point per path step (x, y) */
 };
 
 struct World {
@@ -364,7 +365,142 @@ struct World {
 }  // namespace
 
 struct orc_map : Map {};
-struct orc_world : World {};
+struct orc_world : World {
+    int smoothing = 0;
+};
+
+namespace {
+
+/* ---- path smoothing: portals of the corridor, then the simple stupid funnel
+ * (M. Mononen, 2010).  twice the signed area of (a, b, c), > 0 when c is left
+ * of a -> b; every product and difference rounded to binary32 on its own. */
+float orient2(float ax, float ay, float bx, float by, float cx, float cy) {
+    float ux = bx - ax, uy = by - ay;
+    float vx = cx - ax, vy = cy - ay;
+    float p1 = ux * vy;
+    float p2 = vx * uy;
+    return p1 - p2;
+}
+
+/* portals 0..L+1: the start point, the shared edges (left, right as seen from
+ * the earlier triangle's centroid towards the later one's), the end point */
+void corridor(const Map& m, int start_tri, const std::vector<int>& path, float sx, float sy, float ex, float ey,
+              std::vector<float>& lx, std::vector<float>& ly, std::vector<float>& rx, std::vector<float>& ry) {
+    const int L = (int)path.size();
+    lx.assign(L + 2, 0);
+    ly.assign(L + 2, 0);
+    rx.assign(L + 2, 0);
+    ry.assign(L + 2, 0);
+    lx[0] = rx[0] = sx;
+    ly[0] = ry[0] = sy;
+    lx[L + 1] = rx[L + 1] = ex;
+    ly[L + 1] = ry[L + 1] = ey;
+    for (int k = 1; k <= L; k++) {
+        const int u = k == 1 ? start_tri : path[k - 2], v = path[k - 1];
+        const float* A = &m.t[6 * (size_t)u];
+        const float* B = &m.t[6 * (size_t)v];
+        float sh[4];
+        int cnt = 0;
+        for (int a = 0; a < 3; a++) {
+            bool in_b = false;
+            for (int b = 0; b < 3; b++) in_b = in_b || (A[2 * a] == B[2 * b] && A[2 * a + 1] == B[2 * b + 1]);
+            if (in_b && cnt < 2) {
+                sh[2 * cnt] = A[2 * a];
+                sh[2 * cnt + 1] = A[2 * a + 1];
+            }
+            if (in_b) cnt++;
+        }
+        if (cnt < 2) {
+            lx[k] = rx[k] = m.cx[v];
+            ly[k] = ry[k] = m.cy[v];
+            continue;
+        }
+        const bool first_left = orient2(m.cx[u], m.cy[u], m.cx[v], m.cy[v], sh[0], sh[1]) > 0.0f;
+        const int li = first_left ? 0 : 1, ri = 1 - li;
+        lx[k] = sh[2 * li];
+        ly[k] = sh[2 * li + 1];
+        rx[k] = sh[2 * ri];
+        ry[k] = sh[2 * ri + 1];
+    }
+}
+
+/* steering point of each path step: the first funnel corner at a portal index
+ * past the step's portal (step k crosses portal k + 1) */
+void funnel_points(const Map& m, Agent& ag) {
+    const int L = (int)ag.path.size();
+    std::vector<float> lx, ly, rx, ry;
+    corridor(m, ag.cur, ag.path, ag.px, ag.py, ag.tx, ag.ty, lx, ly, rx, ry);
+    std::vector<float> cx, cy;
+    std::vector<int> ci;  /* corners and their portal indices */
+    float apx = ag.px, apy = ag.py, flx = apx, fly = apy, frx = apx, fry = apy;
+    int apex = 0, lft = 0, rgt = 0;
+    int guard = 0;
+    const int max_guard = 4 * (L + 2) + 16;
+    bool capped = false;
+    int k = 1;
+    while (k <= L + 1) {
+        if (++guard > max_guard) {
+            capped = true;
+            break;
+        }
+        bool restart = false;
+        if (orient2(apx, apy, frx, fry, rx[k], ry[k]) >= 0.0f) {
+            if ((apx == frx && apy == fry) || orient2(apx, apy, flx, fly, rx[k], ry[k]) < 0.0f) {
+                frx = rx[k];
+                fry = ry[k];
+                rgt = k;
+            } else {
+                cx.push_back(flx);
+                cy.push_back(fly);
+                ci.push_back(lft);
+                apx = flx;
+                apy = fly;
+                apex = lft;
+                restart = true;
+            }
+        }
+        if (!restart && orient2(apx, apy, flx, fly, lx[k], ly[k]) <= 0.0f) {
+            if ((apx == flx && apy == fly) || orient2(apx, apy, frx, fry, lx[k], ly[k]) > 0.0f) {
+                flx = lx[k];
+                fly = ly[k];
+                lft = k;
+            } else {
+                cx.push_back(frx);
+                cy.push_back(fry);
+                ci.push_back(rgt);
+                apx = frx;
+                apy = fry;
+                apex = rgt;
+                restart = true;
+            }
+        }
+        if (restart) {
+            flx = frx = apx;
+            fly = fry = apy;
+            lft = rgt = apex;
+            k = apex + 1;
+        } else {
+            k++;
+        }
+    }
+    ag.wp.assign(2 * (size_t)L, 0.0f);
+    size_t c = 0;
+    for (int step = 0; step < L; step++) {
+        while (c < ci.size() && ci[c] < step + 1) c++;
+        if (c < ci.size()) {
+            ag.wp[2 * step] = cx[c];
+            ag.wp[2 * step + 1] = cy[c];
+        } else if (capped) {
+            ag.wp[2 * step] = m.cx[ag.path[step]];
+            ag.wp[2 * step + 1] = m.cy[ag.path[step]];
+        } else {
+            ag.wp[2 * step] = ag.tx;
+            ag.wp[2 * step + 1] = ag.ty;
+        }
+    }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -546,6 +682,7 @@ orc_world* orc_world_create(const orc_map* m, int agents_max, float radius, floa
 }
 
 void orc_world_destroy(orc_world* w) { delete w; }
+void orc_world_set_smoothing(orc_world* w, int on) { w->smoothing = on ? 1 : 0; }
 int orc_world_count(const orc_world* w) { return (int)w->a.size(); }
 
 int orc_world_add_agent(orc_world* w, float x, float y) {
@@ -615,6 +752,11 @@ void orc_world_step(orc_world* w, float dt, int threads) {
     std::vector<int> mv;
     for (int i = 0; i < n; i++)
         if (A[i].state == MOVE) mv.push_back(i);
+    /* path smoothing: steering points of the paths that start this frame,
+     * from the agents' positions at the frame's start */
+    if (w->smoothing)
+        for (int i : mv)
+            if (A[i].step_idx == -1 && !A[i].path.empty()) funnel_points(m, A[i]);
 
     /* 3. searches + path build (PathFinder.h:253-307) */
     std::vector<SearchScratch> scratch(threads);
@@ -759,14 +901,29 @@ void orc_world_step(orc_world* w, float dt, int threads) {
         if (ag.step_idx == -1) {
             ag.step_idx = 0;
             ag.step_node = ag.path[0];
-            ag.sx = m.cx[ag.step_node];
-            ag.sy = m.cy[ag.step_node];
+            ag.sx = w->smoothing ? ag.wp[0] : m.cx[ag.step_node];
+            ag.sy = w->smoothing ? ag.wp[1] : m.cy[ag.step_node];
             continue;
         }
-        if (!point_in_tri(&m.t[6 * ag.step_node], ag.px, ag.py)) continue;
-        ag.cur = ag.step_node;
+        const bool inside = point_in_tri(&m.t[6 * ag.step_node], ag.px, ag.py);
+        bool at_point = false; /* path smoothing: the steering point reached */
+        if (w->smoothing && !inside) {
+            float dx = ag.sx - ag.px, dy = ag.sy - ag.py;
+            float dxx = dx * dx, dyy = dy * dy;
+            at_point = std::sqrt(dxx + dyy) <= arrive;
+        }
+        if (!inside && !at_point) continue;
         int L = (int)ag.path.size();
-        if (ag.step_idx < L) ag.step_idx += 1;
+        if (inside) {
+            ag.cur = ag.step_node;
+            if (ag.step_idx < L) ag.step_idx += 1;
+        } else {
+            /* skip the steps that steer to the point just reached */
+            while (ag.step_idx < L && ag.wp[2 * ag.step_idx] == ag.sx && ag.wp[2 * ag.step_idx + 1] == ag.sy) {
+                ag.cur = ag.path[ag.step_idx];
+                ag.step_idx++;
+            }
+        }
         if (ag.step_idx == L) {
             float dx = ag.tx - ag.px, dy = ag.ty - ag.py;
             float dxx = dx * dx, dyy = dy * dy;
@@ -778,8 +935,8 @@ void orc_world_step(orc_world* w, float dt, int threads) {
             }
         } else {
             ag.step_node = ag.path[ag.step_idx];
-            ag.sx = m.cx[ag.step_node];
-            ag.sy = m.cy[ag.step_node];
+            ag.sx = w->smoothing ? ag.wp[2 * ag.step_idx] : m.cx[ag.step_node];
+            ag.sy = w->smoothing ? ag.wp[2 * ag.step_idx + 1] : m.cy[ag.step_node];
         }
     }
 }

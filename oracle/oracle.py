@@ -58,6 +58,7 @@ def load():
         "orc_queue_sim": (C.c_int, [F, I, I, C.c_int, I, C.c_int, C.c_int, I, I]),
         "orc_bfs_hops": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
         "orc_dijkstra_len": (C.c_double, [C.c_void_p, C.c_int, C.c_int]),
+        "orc_world_set_smoothing": (None, [C.c_void_p, C.c_int]),
         "orc_path_len": (C.c_double, [C.c_void_p, C.c_int, I, C.c_int]),
         "orc_world_create": (C.c_void_p, [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
                                           C.c_float]),
@@ -174,6 +175,9 @@ class OWorld:
         if getattr(self, "h", None):
             self.lib.orc_world_destroy(self.h)
             self.h = None
+
+    def set_smoothing(self, on: bool):
+        self.lib.orc_world_set_smoothing(self.h, 1 if on else 0)
 
     def add_agent(self, x, y):
         return self.lib.orc_world_add_agent(self.h, float(x), float(y))

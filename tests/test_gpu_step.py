@@ -10,12 +10,13 @@ from gpu_util import close_rel
 pytestmark = pytest.mark.gpu
 
 
-def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None, vm=0):
+def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None, vm=0, smoothing=False):
     g, starts, rng = S.make_world(scn, mode=mode, agents=agents, threads_per_agent=T, queue_capacity=Cap,
-                                  parallel_agents=P, visited_mode=vm)
+                                  parallel_agents=P, visited_mode=vm, path_smoothing=smoothing)
     om = oracle_mod.OMap(g.map_nodes())
     ow = oracle_mod.OWorld(om, agents, scn.radius, scn.speed, P or agents, T or scn.threads_per_agent,
                            Cap or scn.queue_capacity, scn.heuristic_k)
+    ow.set_smoothing(smoothing)
     for p in starts:
         assert ow.add_agent(p[0], p[1]) >= 0
     return g, ow, rng
@@ -107,3 +108,41 @@ def test_zigzag_reference_driver(oracle_mod):
     for i, p in enumerate(tp):
         ow.set_target(i, p[0], p[1])
     run(g, ow, scn, 60, rng, check_every=20)
+
+
+@pytest.mark.parametrize("mode", [G.MODE_BATCHED, G.MODE_PLAIN])
+def test_path_smoothing_against_oracle(oracle_mod, mode):
+    # opt-in funnel corners instead of centroids: same triangle paths, agents
+    # steer to the corners; device and oracle funnels agree exactly
+    scn = S.cfg2()
+    g, ow, rng = make_pair(oracle_mod, scn, 512, mode=mode, smoothing=True)
+    d = run(g, ow, scn, 250, rng, retarget_every=100, check_every=25)
+    # steering points lie on corridor vertices or at the target
+    tri = g.map_nodes()
+    verts = {tuple(np.float32(v)) for t in tri for v in (t["P1"], t["P2"], t["P3"])}
+    moving = np.nonzero(d["state"] == G.EAgentState.Move)[0]
+    on_vertex = sum(tuple(np.float32(d["step_pos"][i])) in verts for i in moving)
+    assert len(moving) > 50 and on_vertex > 0
+
+
+def test_path_smoothing_shortens_routes(oracle_mod):
+    # agents that steer through funnel corners arrive no later than agents
+    # that walk centroid to centroid (same targets, no other agents nearby)
+    scn = S.cfg2()
+    times = {}
+    for smooth in (False, True):
+        g, starts, rng = S.make_world(scn, agents=16, path_smoothing=smooth)
+        tp = S.free_points(g, scn, 16, np.random.default_rng(41))
+        g.set_targets(np.arange(16), tp)
+        done = np.full(16, -1)
+        for k in range(60 * 120):
+            g.AsyncStep(1.0)
+            g.WaitStepEnd()
+            _, st = g.agents()
+            newly = (st == G.EAgentState.Idle) & (done < 0) & (k > 0)
+            done[newly] = k
+            if (done >= 0).all():
+                break
+        times[smooth] = done
+    assert (times[True] >= 0).all() and (times[False] >= 0).all()
+    assert times[True].sum() <= times[False].sum()
