@@ -151,8 +151,10 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
 // VM: visited placement (1 shared-memory bitmap, 2 stamped records, 3 global
 // bitmap).  In modes 1 and 3 a bit set by one thread is seen by the others
 // after the next __syncwarp (bar.warp.sync orders memory among its threads).
+// At most 80 registers (three 256-thread blocks per SM): 24 resident warps
+// per SM instead of 20 for the T >= 16 instances, for a few spilled words.
 template <int T, int VM>
-__global__ void __launch_bounds__(256) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
+__global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
     constexpr bool SMEMV = VM == 1;  // bitmap in shared memory
     constexpr bool BMV = VM != 2;    // visited state in a bitmap (shared or global)
     extern __shared__ __align__(16) unsigned char smem[];
