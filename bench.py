@@ -333,7 +333,13 @@ def serving(rates, duration_s: float, n_scenes: int = 8, agents: int = 8192):
             if now >= nxt:
                 f0 = clock_ns()
                 w.AsyncStep(1.0 / 60.0)
-                w.serve_poll()
+                while not w.step_ready():  # keep admitting while the frame runs
+                    now = clock_ns()
+                    j = int(np.searchsorted(arr_ns, now, side="right"))
+                    if j > k:
+                        w.serve_submit(ids[k:j], pos[k:j], arr_ns[k:j])
+                        k = j
+                    w.serve_poll()
                 w.WaitStepEnd()
                 steps.append((clock_ns() - f0) * 1e-6)
                 nxt += frame_ns

@@ -137,6 +137,7 @@ SIGNATURES = {
     "gmapf_map_save": (C.c_int, [P, C.c_char_p]),
     "gmapf_map_load": (C.c_int, [P, C.c_char_p]),
     "gmapf_fill_map_end_cached": (C.c_int, [P, C.c_char_p, I32P]),
+    "gmapf_step_ready": (C.c_int32, [P]),
     "gmapf_serve_start": (C.c_int, [P, C.c_int32]),
     "gmapf_serve_submit": (C.c_int, [P, I32P, V2P, C.c_int32, C.POINTER(C.c_int64)]),
     "gmapf_serve_poll": (C.c_int, [P]),

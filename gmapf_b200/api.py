@@ -165,6 +165,10 @@ class GMAPF:
     def AsyncStep(self, delta_time: float) -> None:
         self._check(self._lib.gmapf_async_step(self._h, float(delta_time)))
 
+    def step_ready(self) -> bool:
+        """True when no step runs or its device work is done (WaitStepEnd will not block)."""
+        return bool(self._lib.gmapf_step_ready(self._h))
+
     def WaitStepEnd(self) -> None:
         self._check(self._lib.gmapf_wait_step_end(self._h))
 

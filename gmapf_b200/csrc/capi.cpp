@@ -511,6 +511,14 @@ gmapf_status gmapf_wait_step_end(gmapf_ctx* ctx) {
     return GMAPF_OK;
 }
 
+int32_t gmapf_step_ready(gmapf_ctx* ctx) {
+    if (!ctx) return 1;
+    if (ctx->world) ctx = ctx->world;
+    Context& c = ctx->c;
+    if (!c.step_going) return 1;
+    return device_step_ready(c) ? 1 : 0;
+}
+
 gmapf_status gmapf_get_agent_pos(gmapf_ctx* ctx, int32_t id, gmapf_v2* out) {
     NEED_CTX(ctx);
     Context& c = ctx->c;

@@ -365,6 +365,7 @@ int device_start(Context& c, std::string& err) {
     CK(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&d.stream2, cudaStreamNonBlocking));
     for (auto& e : d.ev) CK(cudaEventCreate(&e));
+    CK(cudaEventCreateWithFlags(&d.frame_done, cudaEventDisableTiming));
 
     const HostMap& m = c.map;
     const int n = m.n;
@@ -510,6 +511,8 @@ void device_free(Context& c) {
     d.allocs.clear();
     for (auto& e : d.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
+    if (d.frame_done) cudaEventDestroy(d.frame_done);
+    d.frame_done = nullptr;
     if (d.stream) cudaStreamDestroy(d.stream);
     if (d.stream2) cudaStreamDestroy(d.stream2);
     d.stream = d.stream2 = nullptr;
@@ -601,7 +604,15 @@ int device_async_step(Context& c, float dt, std::string& err) {
         CK(cudaMemcpyAsync(c.h_stats, d.stats, sizeof(unsigned long long) * ST_COUNT, cudaMemcpyDeviceToHost, s));
         if (timing) CK(cudaEventRecord(d.ev[4], s));
     }
+    CK(cudaEventRecord(d.frame_done, s));
     return GMAPF_OK;
+}
+
+bool device_step_ready(Context& c) {
+    const cudaError_t e = cudaEventQuery(c.dev.frame_done);
+    if (e == cudaErrorNotReady) return false;
+    cudaGetLastError();
+    return true;  // finished, or failed: WaitStepEnd reports it
 }
 
 int device_wait_step(Context& c, std::string& err) {

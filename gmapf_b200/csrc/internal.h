@@ -274,6 +274,7 @@ struct Device {
     float graph_dt = -1.0f;
     // events
     cudaEvent_t ev[8] = {};
+    cudaEvent_t frame_done = nullptr;  // recorded after each frame's work (step-ready query)
     std::vector<void*> allocs;
 };
 
@@ -349,6 +350,7 @@ int device_start(Context& c, std::string& err);
 void device_free(Context& c);
 int device_async_step(Context& c, float dt, std::string& err);
 int device_wait_step(Context& c, std::string& err);
+bool device_step_ready(Context& c);
 int device_search_batch(Context& c, const int* d_starts, const int* d_targets, int n, int* d_found,
                         int* d_lens, int* d_paths, long long path_stride, gmapf_step_stats* st,
                         std::string& err);

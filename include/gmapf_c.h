@@ -170,6 +170,11 @@ gmapf_status gmapf_manual_start(gmapf_ctx* ctx);
 gmapf_status gmapf_async_step(gmapf_ctx* ctx, float delta_time);
 /* GMAPF::WaitStepEnd()                   -- src/GMAPF.cu:291-314 */
 gmapf_status gmapf_wait_step_end(gmapf_ctx* ctx);
+/* No counterpart in the reference: 1 when no step is running or the running
+ * step's device work has finished (gmapf_wait_step_end will not block), 0
+ * while it runs.  Lets a caller keep serving or preparing input during a
+ * step; the step's results still appear only through gmapf_wait_step_end. */
+int32_t gmapf_step_ready(gmapf_ctx* ctx);
 
 /* GMAPF::GetAgentPos(int)                -- src/GMAPF.cu:316-319 */
 gmapf_status gmapf_get_agent_pos(gmapf_ctx* ctx, int32_t agent_id, gmapf_v2* out);

@@ -146,3 +146,19 @@ def test_path_smoothing_shortens_routes(oracle_mod):
         times[smooth] = done
     assert (times[True] >= 0).all() and (times[False] >= 0).all()
     assert times[True].sum() <= times[False].sum()
+
+
+def test_step_ready_tracks_the_running_step(oracle_mod):
+    import time
+    scn = S.cfg2()
+    g, ow, rng = make_pair(oracle_mod, scn, 512)
+    assert g.step_ready()  # nothing running
+    retarget(g, ow, scn, np.arange(512), rng)
+    g.AsyncStep(scn.dt)
+    t_end = time.time() + 20
+    while not g.step_ready():
+        assert time.time() < t_end
+    g.WaitStepEnd()
+    assert g.step_ready()
+    ow.step(scn.dt, 8)
+    compare(g, ow, 0)
