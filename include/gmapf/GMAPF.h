@@ -140,14 +140,85 @@ public:
 
     void ProfilerDump() const { check(gmapf_profiler_dump(_ctx)); }
 
+    // ---- extensions (no counterpart in the reference; see gmapf_c.h) ----
+    // step form, visited placement, autotuner, path smoothing (before the start)
+    void SetOptions(const gmapf_options& o) { check(gmapf_set_options(_ctx, &o)); }
+    gmapf_options Options() const {
+        gmapf_options o{};
+        check(gmapf_get_options(_ctx, &o));
+        return o;
+    }
+    // FillMapEnd through a navmesh cache file; returns true when the cache was used
+    bool FillMapEndCached(const std::string& path) {
+        int32_t hit = 0;
+        check(gmapf_fill_map_end_cached(_ctx, path.c_str(), &hit));
+        return hit != 0;
+    }
+    void MapSave(const std::string& path) const { check(gmapf_map_save(_ctx, path.c_str())); }
+    void MapLoad(const std::string& path) { check(gmapf_map_load(_ctx, path.c_str())); }
+    // true when no step runs or its device work is done (WaitStepEnd will not block)
+    bool StepReady() const { return gmapf_step_ready(_ctx) != 0; }
+    // serving: retargets searched as soon as they are submitted
+    void ServeStart(int maxInFlight = 0) { check(gmapf_serve_start(_ctx, maxInFlight)); }
+    void ServeSubmit(const std::vector<int>& agentIds, const std::vector<V2Float>& targets) {
+        if (agentIds.size() != targets.size()) throw Error(GMAPF_E_INVALID_ARG, "ids and targets differ in length");
+        check(gmapf_serve_submit(_ctx, agentIds.data(), reinterpret_cast<const gmapf_v2*>(targets.data()),
+                                 (int32_t)agentIds.size(), nullptr));
+    }
+    void ServePoll() { check(gmapf_serve_poll(_ctx)); }
+    void ServeDrain(float timeoutSeconds = 60.0f) { check(gmapf_serve_drain(_ctx, timeoutSeconds)); }
+    gmapf_serve_stats ServeStats(bool reset = false) {
+        gmapf_serve_stats st{};
+        check(gmapf_serve_get_stats(_ctx, &st, reset ? 1 : 0));
+        return st;
+    }
+
     // the C context, for the extensions in gmapf_c.h
     gmapf_ctx* handle() const { return _ctx; }
 
-private:
-    gmapf_ctx* _ctx = nullptr;
     static void check(gmapf_status s) {
         if (s != GMAPF_OK) throw Error(s, std::string("[gmapf] ") + gmapf_last_error());
     }
+
+private:
+    gmapf_ctx* _ctx = nullptr;
+};
+
+// Several scenes stepped as one (gmapf_batch_*): each scene is a GMAPF that
+// was initialised, filled and given its agents; afterwards the scenes keep
+// their per-agent calls (SetAgentTargPos, GetAgentPos, GetAgentState, ...)
+// with their own ids, and frames run here.  The scenes must outlive the batch.
+class SceneBatch {
+public:
+    explicit SceneBatch(const std::vector<GMAPF*>& scenes, const gmapf_options* options = nullptr) {
+        std::vector<gmapf_ctx*> h;
+        for (GMAPF* g : scenes) h.push_back(g->handle());
+        GMAPF::check(gmapf_batch_create(h.data(), (int32_t)h.size(), options, &_b));
+    }
+    SceneBatch(const SceneBatch&) = delete;
+    SceneBatch& operator=(const SceneBatch&) = delete;
+    ~SceneBatch() { gmapf_batch_destroy(_b); }
+
+    void ManualStart() { GMAPF::check(gmapf_manual_start(world())); }
+    void AsyncStep(float deltaTime) { GMAPF::check(gmapf_async_step(world(), deltaTime)); }
+    void WaitStepEnd() { GMAPF::check(gmapf_wait_step_end(world())); }
+    bool StepReady() const { return gmapf_step_ready(world()) != 0; }
+    // serving on the whole batch (agent ids global: see SceneBase)
+    void ServeStart(int maxInFlight = 0) { GMAPF::check(gmapf_serve_start(world(), maxInFlight)); }
+    void ServeDrain(float timeoutSeconds = 60.0f) { GMAPF::check(gmapf_serve_drain(world(), timeoutSeconds)); }
+    gmapf_serve_stats ServeStats(bool reset = false) {
+        gmapf_serve_stats st{};
+        GMAPF::check(gmapf_serve_get_stats(world(), &st, reset ? 1 : 0));
+        return st;
+    }
+    // first global agent id and triangle id of a scene
+    void SceneBase(int scene, int* agentBase, int* nodeBase) const {
+        GMAPF::check(gmapf_batch_scene_base(_b, scene, agentBase, nodeBase));
+    }
+    gmapf_ctx* world() const { return gmapf_batch_world(_b); }
+
+private:
+    gmapf_batch* _b = nullptr;
 };
 
 }  // namespace gmapf

@@ -2,6 +2,9 @@
 //   wrapper_demo cpu   lifecycle and error rules, no GPU needed
 //   wrapper_demo gpu   zig-zag map, agents in a row heading north, N steps;
 //                      prints "agent x y state" lines for the oracle check
+//   wrapper_demo batch the same as two scenes of one SceneBatch (different
+//                      radii), then served retargets on one scene;
+//                      prints "scene s agent x y state" lines and the counts
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -35,7 +38,7 @@ static Config config(int agents) {
 }
 
 int main(int argc, char** argv) {
-    const bool gpu = argc > 1 && std::strcmp(argv[1], "gpu") == 0;
+    const bool gpu = argc > 1 && (std::strcmp(argv[1], "gpu") == 0 || std::strcmp(argv[1], "batch") == 0);
     if (!gpu) {
         GMAPF g;
         g.Init(config(8));
@@ -56,6 +59,52 @@ int main(int argc, char** argv) {
         const V2Float& p = g.GetAgentPos(id);
         std::printf("cpu ok thrown=%d id=%d pos=%g,%g state=%d\n", thrown, id, p.X, p.Y, (int)g.GetAgentState(id));
         return thrown == 2 ? 0 : 1;
+    }
+    if (std::strcmp(argv[1], "batch") == 0) {
+        const int A = 128, steps = 120;
+        GMAPF a, b;
+        Config ca = config(A), cb = config(A);
+        cb.AgentRadius = 1.5f;
+        a.Init(ca);
+        b.Init(cb);
+        zigzag(a);
+        zigzag(b);
+        for (int i = 0; i < A; i++) {
+            a.AddAgent({i / 5.0f + 1.0f, 1.0f});
+            b.AddAgent({i / 4.0f + 2.0f, 3.0f});
+        }
+        for (int i = 0; i < A; i++) {
+            a.SetAgentTargetPos(i, {i / 5.0f + 1.0f, 950.0f});
+            b.SetAgentTargetPos(i, {990.0f - i / 4.0f, 600.0f});
+        }
+        SceneBatch batch({&a, &b});
+        batch.ManualStart();
+        for (int s = 0; s < steps; s++) {
+            batch.AsyncStep(1.0f / 60.0f);
+            batch.WaitStepEnd();
+        }
+        GMAPF* sc[2] = {&a, &b};
+        for (int k = 0; k < 2; k++)
+            for (int i = 0; i < A; i++) {
+                const V2Float& p = sc[k]->GetAgentPos(i);
+                std::printf("scene %d agent %d %.9g %.9g %d\n", k, i, p.X, p.Y, (int)sc[k]->GetAgentState(i));
+            }
+        // served retargets through scene b's own ids
+        batch.ServeStart();
+        std::vector<int> ids;
+        std::vector<V2Float> to;
+        for (int i = 0; i < 16; i++) {
+            ids.push_back(i);
+            to.push_back({50.0f + i, 150.0f});
+        }
+        b.ServeSubmit(ids, to);
+        batch.ServeDrain();
+        batch.AsyncStep(1.0f / 60.0f);
+        batch.WaitStepEnd();
+        const gmapf_serve_stats st = batch.ServeStats();
+        std::printf("served completed=%lld found=%lld applied=%lld\n", (long long)st.completed, (long long)st.found,
+                    (long long)st.applied);
+        return 0;
     }
     const int A = 256, steps = 120;
     GMAPF g;

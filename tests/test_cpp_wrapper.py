@@ -57,3 +57,35 @@ def test_cpp_wrapper_run_matches_oracle(demo, oracle_mod):
     o = ow.get()
     assert np.array_equal(got_state, o["state"])
     assert np.allclose(got_pos, o["pos"], rtol=1e-4, atol=1e-4, equal_nan=True)
+
+
+@pytest.mark.gpu
+def test_cpp_scene_batch_matches_oracle(demo, oracle_mod):
+    import gmapf_b200 as G
+    from gmapf_b200 import scenarios as S
+    r = subprocess.run([str(demo), "batch"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    rows = [ln.split() for ln in r.stdout.splitlines() if ln.startswith("scene ")]
+    assert "served completed=16 found=16 applied=16" in r.stdout
+    g = G.GMAPF()
+    g.Init(G.make_config(4, 2, 1, 4, 4, 16))
+    S.build_map(g, S.zigzag())
+    om = oracle_mod.OMap(g.map_nodes())
+    A = 128
+    f32 = np.float32
+    for k, radius in enumerate([2.0, 1.5]):
+        ow = oracle_mod.OWorld(om, A, radius, 1.0, A, 4, 16, 1.0)
+        for i in range(A):  # the demo's float arithmetic
+            x0 = f32(i) / f32(5) + f32(1) if k == 0 else f32(i) / f32(4) + f32(2)
+            assert ow.add_agent(x0, f32(1) if k == 0 else f32(3)) == i
+        for i in range(A):
+            x1 = f32(i) / f32(5) + f32(1) if k == 0 else f32(990) - f32(i) / f32(4)
+            assert ow.set_target(i, x1, f32(950) if k == 0 else f32(600)) == 0
+        for _ in range(120):
+            ow.step(np.float32(1.0 / 60.0), 8)
+        o = ow.get()
+        mine = [a for a in rows if a[1] == str(k)]
+        pos = np.array([[float(a[4]), float(a[5])] for a in mine], np.float32)
+        st = np.array([int(a[6]) for a in mine])
+        assert np.array_equal(st, o["state"]), f"scene {k} states"
+        assert np.allclose(pos, o["pos"], rtol=1e-4, atol=1e-4, equal_nan=True), f"scene {k} positions"
