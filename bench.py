@@ -490,6 +490,13 @@ def bench_b200(args):
     if rank == 0 and args.quality_sample > 0:
         quality = path_quality(g, args.quality_sample)
 
+    # p99 over many full-retarget frames through the host API (fresh targets each)
+    p99_long = None
+    if rank == 0 and args.p99_frames > 0:
+        wl, _ = run_frames_host(g, target_sets(g, scn, rng, 3 + args.p99_frames, A), 3, args.p99_frames)
+        p99_long = {"frames": args.p99_frames, "p50_step_ms": pct(wl, 50), "p99_step_ms": pct(wl, 99),
+                    "max_step_ms": max(wl)}
+
     # e2e through the host API (fresh targets, same scene)
     sets_e2e = target_sets(g, scn, rng, W + K, A)
     g.reset_profiler()
@@ -591,6 +598,7 @@ def bench_b200(args):
             "plain": plain,
             "batched_config_shape": fixed,
             "path_quality": quality,
+            "e2e_step_ms_over_many_frames": p99_long,
             "batched_over_plain": (e2e_value / plain["value"]) if plain else None,
             "roofline": {"bound": "hbm", "kernel": "k_search", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
@@ -666,6 +674,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=160, help="maze cells per side (160: ~100k triangles)")
     ap.add_argument("--secondary-cells", type=int, default=64, help="also report this maze (0: off)")
+    ap.add_argument("--p99-frames", type=int, default=100,
+                    help="extra full-retarget frames through the host API for the step p50/p99 (0: off)")
     ap.add_argument("--serve-seconds", type=float, default=1.0,
                     help="seconds per arrival rate of the serving configuration (0: off)")
     ap.add_argument("--multi-scene-steps", type=int, default=100,
