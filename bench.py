@@ -33,6 +33,7 @@ import argparse
 import json
 import os
 import statistics
+import tempfile
 import subprocess
 import sys
 import time
@@ -110,7 +111,8 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
+        # the raw samples (GMAPF_CLOCKS_DIR, else the temp directory); the line carries the summary
+        self.path = Path(os.environ.get("GMAPF_CLOCKS_DIR", tempfile.gettempdir())) / f"gmapf_clocks_rank{gpu_index}.csv"
 
     def __enter__(self):
         try:
