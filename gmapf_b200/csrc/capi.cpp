@@ -7,6 +7,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 
 #include "internal.h"
 
@@ -414,7 +415,19 @@ gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id) 
     return GMAPF_OK;
 }
 
+namespace {
+// SetAgentTargPos with the target's triangle already located (node = -2: locate here)
+gmapf_status set_target_located(gmapf_ctx* ctx, int32_t id, float x, float y, int node);
+}  // namespace
+
 gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t id, float x, float y) {
+    return set_target_located(ctx, id, x, y, -2);
+}
+
+}  // extern "C"
+
+namespace {
+gmapf_status set_target_located(gmapf_ctx* ctx, int32_t id, float x, float y, int located) {
     NEED_CTX(ctx);
     Context& c = ctx->c;
     SCENE_WORLD(ctx, w);
@@ -422,7 +435,7 @@ gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t id, float x, float
         return fail(GMAPF_E_STATE, "targets are set through the scene contexts (or gmapf_set_agent_targ_pos_device)");
     if (w) {
         if (id < 0 || id >= c.A) return fail(GMAPF_E_INVALID_ARG, "agent id " + std::to_string(id) + " out of range");
-        const int node = locate_host(c, x, y);
+        const int node = located == -2 ? locate_host(c, x, y) : located;
         if (node < 0) return fail(GMAPF_E_INVALID_POS, "target pos " + v2s(x, y) + " is invalid");
         Context& wc = w->c;
         const int gid = c.agent_base + id, gnode = c.node_base + node;
@@ -436,7 +449,7 @@ gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t id, float x, float
     if (!c.inited) return fail(GMAPF_E_STATE, "not initialized");
     if (!c.map_filled) return fail(GMAPF_E_STATE, "map is not filled");
     if (id < 0 || id >= c.A) return fail(GMAPF_E_INVALID_ARG, "agent id " + std::to_string(id) + " out of range");
-    const int node = locate_host(c, x, y);
+    const int node = located == -2 ? locate_host(c, x, y) : located;
     if (node < 0) return fail(GMAPF_E_INVALID_POS, "target pos " + v2s(x, y) + " is invalid");
     c.m_state[id] = GMAPF_AGENT_SEARCH;
     c.m_targ[id] = gmapf_v2{x, y};
@@ -444,12 +457,29 @@ gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t id, float x, float
     if (c.started) add_dirty(c, id, node, x, y);
     return GMAPF_OK;
 }
+}  // namespace
+
+extern "C" {
 
 gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* pos, int32_t n) {
     NEED_CTX(ctx);
     if (n < 0 || (n > 0 && (!ids || !pos))) return fail(GMAPF_E_INVALID_ARG, "bad bulk arrays");
+    Context& c = ctx->c;
+    std::vector<int> node(n, -2);
+    if (n >= 2048 && c.map_filled && !c.is_world && !c.detached) {
+        // point location is the cost of a large retarget: split it over threads,
+        // then apply in order (the first invalid item stops the call, as before)
+        const LocateGrid g = c.map.view();
+        const int nt = std::max(1, std::min<int>(8, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; t++)
+            th.emplace_back([&, t]() {
+                for (int k = t; k < n; k += nt) node[k] = locate(g, pos[k].X, pos[k].Y);
+            });
+        for (std::thread& x : th) x.join();
+    }
     for (int k = 0; k < n; k++) {
-        gmapf_status s = gmapf_set_agent_targ_pos(ctx, ids[k], pos[k].X, pos[k].Y);
+        gmapf_status s = set_target_located(ctx, ids[k], pos[k].X, pos[k].Y, node[k]);
         if (s != GMAPF_OK) return s;
     }
     return GMAPF_OK;

@@ -142,3 +142,17 @@ def test_navmesh_sizes():
             for j in nb[i]:
                 if j >= 0:
                     assert i in nb[j]
+
+
+def test_bulk_retarget_stops_at_the_first_invalid_point():
+    # large bulks locate in parallel; the items before the first invalid one
+    # are applied, the rest are not (as one call per item would do)
+    scn = S.cfg2()
+    g, starts, rng = S.make_world(scn, agents=5000)
+    tp = S.free_points(g, scn, 5000, rng)
+    tp[3000] = [-10.0, -10.0]
+    with pytest.raises(G.GMAPFError) as e:
+        g.set_targets(np.arange(5000), tp)
+    assert e.value.status_name == "GMAPF_E_INVALID_POS"
+    st = np.array([int(g.GetAgentState(i)) for i in range(5000)])
+    assert np.all(st[:3000] == int(G.EAgentState.Search)) and np.all(st[3000:] == int(G.EAgentState.Idle))
