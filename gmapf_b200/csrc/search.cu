@@ -109,22 +109,32 @@ __device__ __forceinline__ int2 ld_state(const Rec* r) {
     return __ldcg(reinterpret_cast<const int2*>(r));
 }
 
+// a record is one 32-byte (256-bit) access: one L1 pass instead of two
 __device__ __forceinline__ void ld_rec(const Rec* r, int4& a, int4& b) {
-    a = __ldcg(reinterpret_cast<const int4*>(r));
-    b = __ldcg(reinterpret_cast<const int4*>(r) + 1);
+    asm volatile("ld.global.cg.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                 : "l"(r));
 }
 
 __device__ __forceinline__ void st_rec(Rec* r, unsigned stamp, int gd, int a0, int a1, int a2,
                                        int a3, int a4, int a5) {
-    __stcg(reinterpret_cast<int4*>(r), make_int4((int)stamp, gd, a0, a1));
-    __stcg(reinterpret_cast<int4*>(r) + 1, make_int4(a2, a3, a4, a5));
+    asm volatile("st.global.cg.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"((int)stamp), "r"(gd),
+                 "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(a4), "r"(a5)
+                 : "memory");
 }
 
 // 2-bit visited state: bit 0 = claimed, bit 1 = reached from the start
 __device__ __forceinline__ int bm_bits(unsigned w, int n) { return (int)((w >> ((n & 15) << 1)) & 3u); }
 __device__ __forceinline__ int bm_get(const unsigned* bm, int n) { return bm_bits(bm[n >> 4], n); }
+// SHARED: the bitmap is in shared memory; otherwise in global memory, set by
+// a reduction that returns nothing (no register or scoreboard held for it)
+template <bool SHARED>
 __device__ __forceinline__ void bm_set(unsigned* bm, int n, int dir) {
-    atomicOr(bm + (n >> 4), (1u | ((unsigned)dir << 1)) << ((n & 15) << 1));
+    const unsigned bit = (1u | ((unsigned)dir << 1)) << ((n & 15) << 1);
+    if constexpr (SHARED)
+        atomicOr(bm + (n >> 4), bit);
+    else
+        asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(bm + (n >> 4)), "r"(bit) : "memory");
 }
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -261,7 +271,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             uid = node;
             ugd = gd;
             st_rec(rec + node, ep, gd, -1, -1, -1, -1, -1, -1);
-            if (BMV) bm_set(bm, node, gd);
+            if (BMV) bm_set<SMEMV>(bm, node, gd);
         }
         (void)f0;  // the seeds' F never takes part in a comparison: each seed is alone in its queue
         __syncwarp();
@@ -345,7 +355,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     fr[idx] = __float_as_int(F);
                     fr[3 * T + idx] = ngd;
                     fr[6 * T + idx] = n;
-                    if (BMV) bm_set(bm, n, du);
+                    if (BMV) bm_set<SMEMV>(bm, n, du);
                     // ancestors 1..5 of n = ancestors 0..4 of the popped node
                     st_rec(rec + n, ep, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
                 }
