@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
         int tgd = 0, tid = -1;
         bool pop_tail = false;
         bool pv[3] = {false, false, false};  // received items waiting for insertion
+        bool more = false;                   // warp-uniform: the last round claimed more than T nodes
         float pxF[3] = {0.f, 0.f, 0.f};
         int pxg[3] = {0, 0, 0}, pxi[3] = {0, 0, 0};
         if (lane < 2) {  // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
@@ -368,9 +369,11 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             auto deferred_queue_work = [&]() {
                 if (lane < T) {
                     if (pop_tail) qsize--;
-#pragma unroll
-                    for (int j = 0; j < 3; j++)
-                        if (pv[j]) ring_push(ring, qbeg, qsize, C - 1, pxF[j], pxg[j], pxi[j]);
+                    if (pv[0]) ring_push(ring, qbeg, qsize, C - 1, pxF[0], pxg[0], pxi[0]);
+                    if (more) {  // items lane + T, lane + 2T exist only when nwin > T
+                        if (pv[1]) ring_push(ring, qbeg, qsize, C - 1, pxF[1], pxg[1], pxi[1]);
+                        if (pv[2]) ring_push(ring, qbeg, qsize, C - 1, pxF[2], pxg[2], pxi[2]);
+                    }
                     if (qsize > 0) {
                         const int k = ring.at(qbeg + qsize - 1);
                         tF = __int_as_float(ring.word(0)[k]);
@@ -441,7 +444,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     const int nb = __shfl_sync(kFull, r0.y, qq);
                     const int nc = __shfl_sync(kFull, r0.z, qq);
                     int n = sl == 0 ? na : (sl == 1 ? nb : nc);
-                    const bool valid = t < total && cu >= 0 && cu < n_nodes && n >= 0 && n < n_nodes;
+                    const bool valid = t < total && (unsigned)cu < (unsigned)n_nodes && (unsigned)n < (unsigned)n_nodes;
                     if (!valid) n = -1;
                     float cx = 0.f, cy = 0.f;
                     int4 ra = make_int4(0, 0, -1, -1), rb = make_int4(-1, -1, -1, -1);
@@ -485,8 +488,8 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 bool have = lane < T && qsize > 0;
                 float bF = tF;
                 int bg = tgd, bi = tid;
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
+                more = nwin > T;
+                auto take = [&](int j) {
                     const int i = lane + j * T;
                     pv[j] = lane < T && i < nwin;
                     if (pv[j]) {
@@ -501,6 +504,14 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                             bi = pxi[j];
                         }
                     }
+                };
+                take(0);
+                if (more) {
+                    take(1);
+                    take(2);
+                } else {
+                    pv[1] = false;
+                    pv[2] = false;
                 }
                 uid = have ? bi : -1;
                 ugd = bg;
