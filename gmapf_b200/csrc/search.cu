@@ -62,8 +62,8 @@ __device__ __forceinline__ bool key_less(float fa, int ga, int ia, float fb, int
 // A queued node: its key (F, G<<1|dir, id).
 constexpr int kEntryWords = 3;
 
-// Per-lane sorted ring in shared memory: word w of entry k of lane q at
-// [(w*C + k)*T + q].
+// Per-lane sorted ring in shared memory: entry k of lane q is (F, G<<1|dir)
+// as one 8-byte word at fg[k*T + q] and the node id at id[k*T + q].
 struct Ring {
     int* base;
     int T;
@@ -72,7 +72,8 @@ struct Ring {
     __device__ __forceinline__ int at(int k) const {  // k in [0, 2C)
         return (k >= C ? k - C : k) * T + q;
     }
-    __device__ __forceinline__ int* word(int w) const { return base + w * C * T; }
+    __device__ __forceinline__ int2* fg() const { return reinterpret_cast<int2*>(base); }
+    __device__ __forceinline__ int* id() const { return base + 2 * C * T; }
 };
 
 // bounded push (CuQueue.h:33-63 with the (F,G,id) order) into a ring holding
@@ -81,7 +82,8 @@ __device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, in
     if (cap <= 0) return;
     if (size == cap) {
         const int k0 = r.at(beg);
-        if (!key_less(F, gd, id, __int_as_float(r.word(0)[k0]), r.word(1)[k0], r.word(2)[k0]))
+        const int2 e = r.fg()[k0];
+        if (!key_less(F, gd, id, __int_as_float(e.x), e.y, r.id()[k0]))
             return;                            // not below the maximum: dropped
         beg = (beg + 1 == r.C) ? 0 : beg + 1;  // evict the maximum
         size--;
@@ -89,19 +91,17 @@ __device__ __forceinline__ void ring_push(const Ring& r, int& beg, int& size, in
     int i = size - 1;
     while (i >= 0) {
         const int k = r.at(beg + i);
-        const float ef = __int_as_float(r.word(0)[k]);
-        const int eg = r.word(1)[k], ei = r.word(2)[k];
-        if (!key_less(ef, eg, ei, F, gd, id)) break;
+        const int2 e = r.fg()[k];
+        const int ei = r.id()[k];
+        if (!key_less(__int_as_float(e.x), e.y, ei, F, gd, id)) break;
         const int k1 = r.at(beg + i + 1);
-        r.word(0)[k1] = __float_as_int(ef);
-        r.word(1)[k1] = eg;
-        r.word(2)[k1] = ei;
+        r.fg()[k1] = e;
+        r.id()[k1] = ei;
         i--;
     }
     const int k1 = r.at(beg + i + 1);
-    r.word(0)[k1] = __float_as_int(F);
-    r.word(1)[k1] = gd;
-    r.word(2)[k1] = id;
+    r.fg()[k1] = make_int2(__float_as_int(F), gd);
+    r.id()[k1] = id;
     size++;
 }
 
@@ -376,9 +376,10 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     }
                     if (qsize > 0) {
                         const int k = ring.at(qbeg + qsize - 1);
-                        tF = __int_as_float(ring.word(0)[k]);
-                        tgd = ring.word(1)[k];
-                        tid = ring.word(2)[k];
+                        const int2 e = ring.fg()[k];
+                        tF = __int_as_float(e.x);
+                        tgd = e.y;
+                        tid = ring.id()[k];
                     }
                 }
             };
