@@ -20,8 +20,9 @@ namespace gmapf_b200 {
 // are reused across queries and frames without clearing.  `gd` = G << 1 | dir
 // (dir 1 = reached from the start, PathNode::FromStart).  anc[0] is the
 // parent (PathNode::PrevNodeIdx); anc[k] the (k+1)-th ancestor, so a path
-// walk advances six hops per record read.
-struct __align__(16) Rec {
+// walk advances six hops per record read.  One 32-byte sector: it is read
+// and written as a whole (records.cuh).
+struct __align__(32) Rec {
     unsigned stamp;
     int gd;
     int anc[6];

@@ -30,6 +30,7 @@
 #include <string>
 
 #include "internal.h"
+#include "records.cuh"
 
 namespace gmapf_b200 {
 namespace {
@@ -136,8 +137,7 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
             q[2 * C * T + k] = node;
             for (int j = 0; j < 5; j++) q[(3 + j) * C * T + k] = -1;
             size = 1;
-            __stcg(reinterpret_cast<int4*>(rec + node), make_int4((int)ep, lane == 0 ? 1 : 0, -1, -1));
-            __stcg(reinterpret_cast<int4*>(rec + node) + 1, make_int4(-1, -1, -1, -1));
+            st_rec(rec + node, ep, lane == 0 ? 1 : 0, -1, -1, -1, -1, -1, -1);
         }
         __syncwarp();
         int found = 0, mS = 0, gS = 0, mT = 0, gT = 0, rounds = 0;
@@ -212,8 +212,7 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
                     fr[6 * T + idx] = n;
                     fr[9 * T + idx] = cu;
                     for (int j = 0; j < 4; j++) fr[(4 + j) * 3 * T + idx] = ua[j];
-                    __stcg(reinterpret_cast<int4*>(rec + n), make_int4((int)ep, ngd, cu, ua[0]));
-                    __stcg(reinterpret_cast<int4*>(rec + n) + 1, make_int4(ua[1], ua[2], ua[3], ua[4]));
+                    st_rec(rec + n, ep, ngd, cu, ua[0], ua[1], ua[2], ua[3], ua[4]);
                 }
                 nwin += __popc(wm);
                 __syncwarp();
@@ -281,8 +280,8 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
                     out[gS] = x;
                 }
                 while (g > stop && x >= 0 && x < n_nodes) {
-                    const int4 p0 = __ldcg(reinterpret_cast<const int4*>(rec + x));
-                    const int4 p1 = __ldcg(reinterpret_cast<const int4*>(rec + x) + 1);
+                    int4 p0, p1;
+                    ld_rec(rec + x, p0, p1);
                     const int anc[6] = {p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
                     for (int j = 0; j < 6; j++) {
                         const int d = g - 1 - j;

@@ -46,6 +46,7 @@
 #include <mutex>
 
 #include "internal.h"
+#include "records.cuh"
 
 namespace gmapf_b200 {
 
@@ -109,23 +110,10 @@ __device__ __forceinline__ int2 ld_state(const Rec* r) {
     return __ldcg(reinterpret_cast<const int2*>(r));
 }
 
-// a record is one 32-byte (256-bit) access: one L1 pass instead of two
-__device__ __forceinline__ void ld_rec(const Rec* r, int4& a, int4& b) {
-    asm volatile("ld.global.cg.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
-                 : "l"(r));
-}
-
-__device__ __forceinline__ void st_rec(Rec* r, unsigned stamp, int gd, int a0, int a1, int a2,
-                                       int a3, int a4, int a5) {
-    asm volatile("st.global.cg.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"((int)stamp), "r"(gd),
-                 "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(a4), "r"(a5)
-                 : "memory");
-}
-
 // 2-bit visited state: bit 0 = claimed, bit 1 = reached from the start
 __device__ __forceinline__ int bm_bits(unsigned w, int n) { return (int)((w >> ((n & 15) << 1)) & 3u); }
 __device__ __forceinline__ int bm_get(const unsigned* bm, int n) { return bm_bits(bm[n >> 4], n); }
+
 // SHARED: the bitmap is in shared memory; otherwise in global memory, set by
 // a reduction that returns nothing (no register or scoreboard held for it)
 template <bool SHARED>
