@@ -466,9 +466,15 @@ gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, c
     if (n < 0 || (n > 0 && (!ids || !pos))) return fail(GMAPF_E_INVALID_ARG, "bad bulk arrays");
     Context& c = ctx->c;
     std::vector<int> node(n, -2);
-    if (n >= 2048 && c.map_filled && !c.is_world && !c.detached) {
-        // point location is the cost of a large retarget: split it over threads,
-        // then apply in order (the first invalid item stops the call, as before)
+    if (n >= 2048 && c.map_filled && c.started && !c.is_world && !c.detached && !ctx->world) {
+        // point location is the cost of a large retarget: on the device (its own
+        // stream: a running frame is not waited for), then applied in order
+        // below (the first invalid item stops the call)
+        std::string err;
+        const int rc = device_locate_points(c, pos, n, node.data(), err);
+        if (rc) return fail(rc, err);
+    } else if (n >= 2048 && c.map_filled && !c.is_world && !c.detached) {
+        // before start: split it over host threads
         const LocateGrid g = c.map.view();
         const int nt = std::max(1, std::min<int>(8, (int)std::thread::hardware_concurrency()));
         std::vector<std::thread> th;

@@ -516,6 +516,17 @@ void device_free(Context& c) {
     if (d.stream) cudaStreamDestroy(d.stream);
     if (d.stream2) cudaStreamDestroy(d.stream2);
     d.stream = d.stream2 = nullptr;
+    if (d.loc_stream) cudaStreamSynchronize(d.loc_stream), cudaStreamDestroy(d.loc_stream);
+    if (d.loc_pts) cudaFree(d.loc_pts);
+    if (d.loc_node) cudaFree(d.loc_node);
+    if (d.h_loc_pts) cudaFreeHost(d.h_loc_pts);
+    if (d.h_loc_node) cudaFreeHost(d.h_loc_node);
+    d.loc_stream = nullptr;
+    d.loc_pts = nullptr;
+    d.loc_node = nullptr;
+    d.h_loc_pts = nullptr;
+    d.h_loc_node = nullptr;
+    d.loc_cap = 0;
     void* hp[] = {c.h_pos_stage, c.h_state_stage, c.h_dirty, c.h_small, c.h_stats, c.h_step};
     for (void* p : hp)
         if (p) cudaFreeHost(p);
@@ -688,6 +699,44 @@ int device_wait_step(Context& c, std::string& err) {
         err = "device-side check failed (error bits " + std::to_string(e) + ")";
         return GMAPF_E_DEVICE;
     }
+    return GMAPF_OK;
+}
+
+int device_locate_points(Context& c, const gmapf_v2* pts, int n, int* node, std::string& err) {
+    Device& d = c.dev;
+    if (n <= 0) return GMAPF_OK;
+    if (c.scene_par.size() != 1) {
+        err = "device point location needs a single-map context";
+        return GMAPF_E_STATE;
+    }
+    CK(cudaSetDevice(d.device));
+    if (!d.loc_stream) CK(cudaStreamCreateWithFlags(&d.loc_stream, cudaStreamNonBlocking));
+    if (n > d.loc_cap) {
+        cudaFree(d.loc_pts);
+        cudaFree(d.loc_node);
+        cudaFreeHost(d.h_loc_pts);
+        cudaFreeHost(d.h_loc_node);
+        d.loc_pts = nullptr;
+        d.loc_node = nullptr;
+        d.h_loc_pts = nullptr;
+        d.h_loc_node = nullptr;
+        d.loc_cap = 0;
+        const int cap = std::max(n, 4096);
+        CK(cudaMalloc(&d.loc_pts, sizeof(float2) * cap));
+        CK(cudaMalloc(&d.loc_node, sizeof(int) * cap));
+        CK(cudaHostAlloc(&d.h_loc_pts, sizeof(float2) * cap, cudaHostAllocDefault));
+        CK(cudaHostAlloc(&d.h_loc_node, sizeof(int) * cap, cudaHostAllocDefault));
+        d.loc_cap = cap;
+    }
+    static_assert(sizeof(gmapf_v2) == sizeof(float2), "point layout");
+    std::memcpy(d.h_loc_pts, pts, sizeof(float2) * n);
+    CK(cudaMemcpyAsync(d.loc_pts, d.h_loc_pts, sizeof(float2) * n, cudaMemcpyHostToDevice, d.loc_stream));
+    launch_locate_points(d.loc_stream, c.scene_par[0].loc, d.loc_pts, n, d.loc_node);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(d.h_loc_node, d.loc_node, sizeof(int) * n, cudaMemcpyDeviceToHost, d.loc_stream));
+    CK(cudaStreamSynchronize(d.loc_stream));
+    std::memcpy(node, d.h_loc_node, sizeof(int) * n);
+    c.launches += 1;
     return GMAPF_OK;
 }
 

@@ -146,6 +146,8 @@ void launch_compact(cudaStream_t s, int A, int* state, const int* cur, const int
 void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, int* targ_node,
                           float2* targ_pos);
 // device-resident retargets of agents id_base + ids[k], ids[k] in [0, id_count)
+// point location of n points in one map (found ids include g.base; -1: none)
+void launch_locate_points(cudaStream_t s, const LocateGrid& g, const float2* pts, int n, int* out);
 void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int id_base,
                                  int id_count, const ScenePar* sc, const int* agent_scene, int* state,
                                  int* targ_node, float2* targ_pos, int* err);
@@ -277,6 +279,14 @@ struct Device {
     cudaEvent_t ev[8] = {};
     cudaEvent_t frame_done = nullptr;  // recorded after each frame's work (step-ready query)
     std::vector<void*> allocs;
+    // bulk point location (large host retargets), on its own stream so it never
+    // waits behind a running frame; buffers grow to the largest call
+    cudaStream_t loc_stream = nullptr;
+    float2* loc_pts = nullptr;
+    int* loc_node = nullptr;
+    float2* h_loc_pts = nullptr;  // pinned
+    int* h_loc_node = nullptr;    // pinned
+    int loc_cap = 0;
 };
 
 struct Profiler {
@@ -360,6 +370,9 @@ int device_debug_agents(Context& c, gmapf_v2* pos, int* state, int* cur, int* ta
 int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::string& err);
 int device_autotune(Context& c, std::string& err);
 int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
+// the triangle of each of n host points, located on the device with the
+// same rule as the host (single-map context, after start); blocks until done
+int device_locate_points(Context& c, const gmapf_v2* pts, int n, int* node, std::string& err);
 int device_set_targets_device(Context& c, const int* d_ids, const gmapf_v2* d_pos, int n, int id_base,
                               int id_count, std::string& err);
 

@@ -585,6 +585,13 @@ __global__ void k_funnel(MoverParams p) {
     }
 }
 
+// GMAPF.cu:227,244 -> CuNodesMap.h:53-66 for a batch of points: the first
+// containing triangle in ascending id, through the point-location grid
+__global__ void k_locate_points(LocateGrid g, const float2* pts, int n, int* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = locate(g, pts[i].x, pts[i].y);
+}
+
 inline int blocks_for(int n, int bt) { return (n + bt - 1) / bt; }
 
 }  // namespace
@@ -600,6 +607,11 @@ void launch_apply_targets(cudaStream_t s, const int4* recs, int n, int* state, i
                           float2* targ_pos) {
     if (n <= 0) return;
     k_apply_targets<<<blocks_for(n, 256), 256, 0, s>>>(recs, n, state, targ_node, targ_pos);
+}
+
+void launch_locate_points(cudaStream_t s, const LocateGrid& g, const float2* pts, int n, int* out) {
+    if (n <= 0) return;
+    k_locate_points<<<blocks_for(n, 256), 256, 0, s>>>(g, pts, n, out);
 }
 
 void launch_apply_targets_device(cudaStream_t s, const int* ids, const float2* pos, int n, int id_base,
