@@ -155,7 +155,11 @@ gmapf_status gmapf_add_agent(gmapf_ctx* ctx, float x, float y, int32_t* out_id);
 /* GMAPF::SetAgentTargPos(int, V2Float)   -- src/GMAPF.cu:238-253
  * (README.md:78 spells it SetAgentTargetPos; both C++ spellings map here) */
 gmapf_status gmapf_set_agent_targ_pos(gmapf_ctx* ctx, int32_t agent_id, float x, float y);
-/* bulk form of the above: n targets, one call */
+/* bulk form of the above: n targets, one call, the same as n calls in order
+ * (the first invalid position stops it with GMAPF_E_INVALID_POS, the items
+ * before it applied).  From 2,048 targets the points are located on the
+ * device once the context is started (on a stream of their own: a running
+ * step is not waited for), before that on several host threads. */
 gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, const gmapf_v2* pos, int32_t n);
 /* device-resident form: ids and positions already in device memory; the
  * target triangles are located on the device (same rule as the host path).
