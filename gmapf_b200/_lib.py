@@ -128,6 +128,8 @@ SIGNATURES = {
     "gmapf_reset_profiler": (C.c_int, [P]),
     "gmapf_kernel_launches": (C.c_int64, [P]),
     "gmapf_search_shape": (C.c_int, [P, I32P, I32P, I32P, I32P, I32P]),
+    "gmapf_set_tune_cache": (C.c_int, [P, C.c_char_p]),
+    "gmapf_tune_source": (C.c_int, [P, I32P]),
     "gmapf_stream_handle": (C.c_void_p, [P]),
     "gmapf_search_batch_host": (C.c_int, [P, I32P, I32P, C.c_int32, I32P, I32P, I32P, C.c_int32,
                                           C.POINTER(StepStats)]),

@@ -312,6 +312,16 @@ class GMAPF:
         """cudaStream_t of the library (0 before the start)."""
         return self._lib.gmapf_stream_handle(self._h) or 0
 
+    def set_tune_cache(self, path) -> None:
+        """Autotuner cache file (before the start); None turns it off."""
+        self._check(self._lib.gmapf_set_tune_cache(self._h, None if path is None else str(path).encode()))
+
+    def tune_source(self) -> int:
+        """0: the Config's shape, 1: tuned at the start, 2: from the autotuner cache."""
+        v = C.c_int32()
+        self._check(self._lib.gmapf_tune_source(self._h, C.byref(v)))
+        return v.value
+
     def search_shape(self) -> dict:
         v = [C.c_int32() for _ in range(5)]
         self._check(self._lib.gmapf_search_shape(self._h, *[C.byref(x) for x in v]))

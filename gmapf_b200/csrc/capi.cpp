@@ -80,6 +80,7 @@ int add_dirty(Context& c, int id, int node, float x, float y) {
 }
 
 uint64_t cdt_input_hash(const Context& c);  // navmesh files, below
+int autotune_at_start(Context& c, std::string& err);  // autotuner cache, below
 
 gmapf_status start_if_needed(Context& c) {
     if (c.started) return GMAPF_OK;
@@ -91,8 +92,9 @@ gmapf_status start_if_needed(Context& c) {
         return fail(rc, err);
     }
     c.started = true;
+    c.tune_source = 0;
     if (c.opt.autotune) {
-        rc = device_autotune(c, err);
+        rc = autotune_at_start(c, err);
         if (rc) return fail(rc, err);
     }
     return GMAPF_OK;
@@ -282,6 +284,86 @@ uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603u
         h *= 1099511628211ull;
     }
     return h;
+}
+
+// ---- autotuner cache ----------------------------------------------------
+// One text line per tuned (map, GPU, options):
+//   gmapf-tune 1 <key, 16 hex digits> <T> <C> <visited placement> <block>
+// The key hashes the search graph and its geometry, the search parameters and
+// options the tuner reads, the GPU (name, SM count, memory) and this build,
+// so a changed map, GPU, option or library never reuses a stale shape.
+// Unreadable or foreign lines are skipped; the last matching line wins.
+const char kTuneBuild[] = "gmapf-tune 1 " __DATE__ " " __TIME__;
+
+uint64_t tune_key(const Context& c) {
+    const HostMap& m = c.map;
+    uint64_t h = fnv1a(kTuneBuild, sizeof(kTuneBuild));
+    h = fnv1a(&m.n, sizeof(m.n), h);
+    h = fnv1a(m.rows.data(), sizeof(SearchRow) * m.rows.size(), h);
+    h = fnv1a(m.cen.data(), sizeof(float2) * m.cen.size(), h);
+    const int32_t iv[] = {c.cfg.PathFinderParallelAgents, c.cfg.PathFinderThreadsPerAgents,
+                          c.cfg.PathFinderQueueCapacity, c.opt.visited_mode, c.opt.block_threads, c.opt.mode};
+    h = fnv1a(iv, sizeof(iv), h);
+    h = fnv1a(&c.cfg.PathFinderHeuristicK, sizeof(float), h);
+    h = fnv1a(&c.opt.search_mem_budget, sizeof(c.opt.search_mem_budget), h);
+    cudaDeviceProp pr{};
+    if (cudaGetDeviceProperties(&pr, c.dev.device) == cudaSuccess) {
+        h = fnv1a(pr.name, std::strlen(pr.name), h);
+        h = fnv1a(&pr.multiProcessorCount, sizeof(pr.multiProcessorCount), h);
+        h = fnv1a(&pr.totalGlobalMem, sizeof(pr.totalGlobalMem), h);
+    } else {
+        cudaGetLastError();
+    }
+    return h;
+}
+
+bool tune_lookup(const std::string& path, uint64_t key, int v[4]) {
+    std::FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    bool hit = false;
+    char line[256];
+    while (std::fgets(line, sizeof(line), f)) {
+        unsigned long long k = 0;
+        int fmt = 0, T = 0, C = 0, vm = 0, bt = 0;
+        if (std::sscanf(line, "gmapf-tune %d %16llx %d %d %d %d", &fmt, &k, &T, &C, &vm, &bt) != 6) continue;
+        if (fmt != 1 || k != key) continue;
+        const bool t_ok = T == 2 || T == 4 || T == 8 || T == 16 || T == 32;
+        if (!t_ok || C < 1 || vm < 0 || vm > 3 || bt < 0 || bt > 1024) continue;
+        v[0] = T, v[1] = C, v[2] = vm, v[3] = bt;
+        hit = true;
+    }
+    std::fclose(f);
+    return hit;
+}
+
+void tune_store(const std::string& path, uint64_t key, const Context& c) {
+    std::FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return;  // the cache only saves time: a start never fails on it
+    std::fprintf(f, "gmapf-tune 1 %016llx %d %d %d %d\n", (unsigned long long)key, c.T, c.C, c.tuned_vm,
+                 c.tuned_bt);
+    std::fclose(f);
+}
+
+int autotune_at_start(Context& c, std::string& err) {
+    uint64_t key = 0;
+    if (!c.tune_cache.empty()) {
+        key = tune_key(c);
+        int v[4];
+        if (tune_lookup(c.tune_cache, key, v)) {
+            const int rc = device_apply_tuned_shape(c, v[0], v[1], v[2], v[3], err);
+            if (rc == GMAPF_OK) {
+                c.tune_source = 2;
+                return GMAPF_OK;
+            }
+            // the stored shape does not fit this process (memory): tune again
+            err.clear();
+        }
+    }
+    const int rc = device_autotune(c, err);
+    if (rc) return rc;
+    c.tune_source = 1;
+    if (!c.tune_cache.empty()) tune_store(c.tune_cache, key, c);
+    return GMAPF_OK;
 }
 
 uint64_t cdt_input_hash(const Context& c) {
@@ -738,6 +820,23 @@ void* gmapf_stream_handle(gmapf_ctx* ctx) {
     if (ctx && ctx->world) ctx = ctx->world;
     if (!ctx || !ctx->c.started) return nullptr;
     return (void*)ctx->c.dev.stream;
+}
+
+gmapf_status gmapf_set_tune_cache(gmapf_ctx* ctx, const char* path) {
+    NEED_CTX(ctx);
+    Context& c = ctx->c;
+    if (c.started) return fail(GMAPF_E_STATE, "set the autotuner cache before the start");
+    c.tune_cache = path ? path : "";
+    return GMAPF_OK;
+}
+
+gmapf_status gmapf_tune_source(gmapf_ctx* ctx, int32_t* source) {
+    NEED_CTX(ctx);
+    if (!source) return fail(GMAPF_E_INVALID_ARG, "null output pointer");
+    if (ctx->world) ctx = ctx->world;
+    if (!ctx->c.started) return fail(GMAPF_E_STATE, "not started");
+    *source = ctx->c.tune_source;
+    return GMAPF_OK;
 }
 
 gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t* bt, int32_t* vm,

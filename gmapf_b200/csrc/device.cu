@@ -898,6 +898,14 @@ int device_reconfigure_search(Context& c, std::string& err) {
     return alloc_search_state(c, err);
 }
 
+int device_apply_tuned_shape(Context& c, int T, int C, int vm, int bt, std::string& err) {
+    c.T = T;
+    c.C = C;
+    c.tuned_vm = vm;
+    c.tuned_bt = bt;
+    return device_reconfigure_search(c, err);
+}
+
 // Per-map autotuner (batched form): threads per agent T, queue capacity C,
 // visited-state placement and block size.  T and C are parameters of the
 // method itself (README.md:98-101: "picked empirically"), so the tuner keeps

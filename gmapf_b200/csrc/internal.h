@@ -336,6 +336,8 @@ struct Context {
     float K = 1.0f;
     // autotuner's choices where the options leave them open (0: pick by occupancy)
     int tuned_vm = 0, tuned_bt = 0;
+    std::string tune_cache;  // autotuner cache file ("" = none)
+    int tune_source = 0;     // 0 not tuned, 1 tuned at the start, 2 from the cache
     // device
     Device dev;
     Profiler prof;
@@ -369,6 +371,8 @@ int device_debug_agents(Context& c, gmapf_v2* pos, int* state, int* cur, int* ta
                         int* step_node, gmapf_v2* step_pos, int* path_len, std::string& err);
 int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::string& err);
 int device_autotune(Context& c, std::string& err);
+// use a shape the autotuner picked before (T, C, visited placement, block size)
+int device_apply_tuned_shape(Context& c, int T, int C, int vm, int bt, std::string& err);
 int device_upload_batch_io(Context& c, int n, long long path_stride, std::string& err);
 // the triangle of each of n host points, located on the device with the
 // same rule as the host (single-map context, after start); blocks until done

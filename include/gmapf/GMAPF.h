@@ -143,6 +143,14 @@ public:
     // ---- extensions (no counterpart in the reference; see gmapf_c.h) ----
     // step form, visited placement, autotuner, path smoothing (before the start)
     void SetOptions(const gmapf_options& o) { check(gmapf_set_options(_ctx, &o)); }
+    // autotuner cache file (before the start); "" turns it off
+    void SetTuneCache(const std::string& path) { check(gmapf_set_tune_cache(_ctx, path.c_str())); }
+    // 0: the Config's shape, 1: tuned at the start, 2: from the autotuner cache
+    int TuneSource() const {
+        int32_t v = 0;
+        check(gmapf_tune_source(_ctx, &v));
+        return v;
+    }
     gmapf_options Options() const {
         gmapf_options o{};
         check(gmapf_get_options(_ctx, &o));

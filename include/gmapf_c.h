@@ -221,6 +221,16 @@ void* gmapf_stream_handle(gmapf_ctx* ctx);
  * 3 global bitmap) and resident request slots */
 gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t* block_threads,
                                 int32_t* visited_mode, int32_t* slots);
+/* Autotuner cache (no reference counterpart): with a file set, the shape the
+ * autotuner picks for this map, GPU, search parameters and options is kept
+ * there (one text line) and later starts with the same inputs take it from
+ * the file instead of tuning again (the tuning takes seconds on large maps).
+ * Set before the start; NULL or "" turns it off.  A file that cannot be read
+ * or written only costs the time of tuning. */
+gmapf_status gmapf_set_tune_cache(gmapf_ctx* ctx, const char* path);
+/* how the started context's search shape was chosen: 0 the Config's (no
+ * autotune), 1 tuned at the start, 2 taken from the autotuner cache */
+gmapf_status gmapf_tune_source(gmapf_ctx* ctx, int32_t* source);
 
 /* ---- batched query API: searches only, no agents ---- */
 /* Run n independent searches (start/target node ids) with the context's

@@ -144,6 +144,16 @@ def test_navmesh_sizes():
                     assert i in nb[j]
 
 
+def test_tune_cache_is_set_before_the_start(tmp_path):
+    scn = S.cfg1()
+    g, starts, rng = S.make_world(scn, agents=4)
+    g.set_tune_cache(tmp_path / "tune.txt")
+    g.set_tune_cache(None)
+    with pytest.raises(G.GMAPFError) as e:
+        g.tune_source()
+    assert e.value.status_name == "GMAPF_E_STATE"
+
+
 def test_bulk_retarget_stops_at_the_first_invalid_point():
     # large bulks locate in parallel; the items before the first invalid one
     # are applied, the rest are not (as one call per item would do)

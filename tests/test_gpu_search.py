@@ -103,6 +103,39 @@ def test_autotune_keeps_fixed_options(oracle_mod):
     check_batch(oracle_mod, g, s, t, sh["T"], sh["C"])
 
 
+def test_autotune_cache_reuses_the_shape(oracle_mod, tmp_path):
+    path = tmp_path / "tune.txt"
+
+    def started(scn):
+        g = G.GMAPF()
+        g.Init(G.make_config(4, scn.radius, scn.speed, 4, 8, 32, scn.heuristic_k))
+        g.set_options(autotune=True)
+        g.set_tune_cache(path)
+        S.build_map(g, scn)
+        g.ManualStart()
+        return g
+
+    shape = lambda g: {k: v for k, v in g.search_shape().items() if k != "slots"}
+    scn = S.cfg3(cells=24)
+    g1 = started(scn)
+    assert g1.tune_source() == 1
+    assert len(path.read_text().splitlines()) == 1
+    s, t = random_queries(g1, scn, 800, seed=21)
+    r1 = g1.search_batch(s, t, g1.node_count)
+    sh1 = shape(g1)
+    g1.close()
+    path.write_text("not a cache line\n" + path.read_text())  # foreign lines are skipped
+    g2 = started(scn)
+    assert g2.tune_source() == 2 and shape(g2) == sh1
+    r2 = g2.search_batch(s, t, g2.node_count)
+    assert all(np.array_equal(x, y) for x, y in zip(r1[:3], r2[:3]))
+    check_batch(oracle_mod, g2, s, t, sh1["T"], sh1["C"])
+    g2.close()
+    g3 = started(S.cfg3(cells=24, seed=4))  # another map: tuned, a line of its own
+    assert g3.tune_source() == 1
+    assert len(path.read_text().splitlines()) == 3
+
+
 def test_longest_first_order_does_not_change_results(oracle_mod):
     scn = S.cfg3(cells=32)
     go = map_world(scn, T=8, Cap=16, order=True)
