@@ -179,6 +179,33 @@ def measured_traffic(cells: int, T: int, C: int, vm: int, queries_per_step: floa
     return d["bytes_per_query"] * queries_per_step, d["source"]
 
 
+def measured_inst_per_round(cells: int, T: int, C: int, vm: int):
+    """Warp instructions per search round from the committed ncu capture of
+    the full frame (profiles/search_issue.json), or None when no capture
+    matches this workload and shape."""
+    p = ROOT / "profiles" / "search_issue.json"
+    if not p.exists():
+        return None, None
+    d = json.loads(p.read_text()).get(f"maze{cells}_T{T}_C{C}_vm{vm}")
+    if not d:
+        return None, None
+    return d["inst_per_round"], d["source"]
+
+
+def issue_roofline(rounds: int, search_ms: float, ipr, src, sm_mhz, sms: int):
+    """The search kernel against the schedulers' issue rate: instructions
+    (rounds x instructions per round) per second over 4 schedulers x SMs x SM
+    clock (one warp instruction per scheduler per cycle)."""
+    if ipr is None or not search_ms:
+        return None
+    mhz = sm_mhz or 1965.0
+    achieved = rounds * ipr / (search_ms / 1e3) / 1e9
+    peak = 4 * sms * mhz / 1e3
+    return {"bound": "issue", "kernel": "k_search", "achieved": achieved, "peak": peak,
+            "unit": "G warp instructions/s", "frac": achieved / peak, "inst_per_round": ipr,
+            "inst_source": src, "peak_basis": f"4 schedulers x {sms} SMs x {mhz:.0f} MHz (sampled SM clock)"}
+
+
 def algorithmic_bytes(st: dict, n_nodes: int) -> float:
     """Search bytes by the fixed per-unit definitions: per expansion 12 B of
     adjacency plus 24 B per neighbour (centroid, visited word, record); per
@@ -515,6 +542,8 @@ def bench_b200(args):
     achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic, traffic_src = measured_traffic(args.cells, Tb, Cb, shape["visited_mode"], queries / max(1, K))
+    ipr, ipr_src = measured_inst_per_round(args.cells, Tb, Cb, shape["visited_mode"])
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
 
     # batched form at the Config's own shape (same arithmetic as the plain form)
     fixed = None
@@ -569,6 +598,7 @@ def bench_b200(args):
 
     if rank == 0:
         st_sum = {k: sum(s[k] for s in dstats) for k in ["requests", "found", "expansions", "rounds", "claims"]}
+        clocks = clk.summary()
         line = {
             "metric": METRIC,
             "value": value,
@@ -607,12 +637,14 @@ def bench_b200(args):
                          "traffic": traffic, "traffic_source": traffic_src,
                          "search_ms_per_step": statistics.mean(search_ms),
                          "algorithmic_bytes_per_step": statistics.mean(ab)},
+            "roofline_issue": issue_roofline(st_sum["rounds"], sum(search_ms), ipr, ipr_src, clocks.get("sm_mhz"),
+                                             sms),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "path queries/s", "h2d_bytes_per_step": 16 * A + 4,
                     "d2h_bytes_per_step": 12 * A + 64 + 8 * 8, "p99_step_ms": pct(wall, 99),
                     "p50_step_ms": pct(wall, 50)},
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "secondary": secondary,
             "multi_scene": multi,
             "serving": serve,
