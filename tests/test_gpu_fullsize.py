@@ -1,0 +1,69 @@
+"""The bench frame's size and shape: the ~100k-triangle maze (160x160 cells,
+101,698 triangles), 16,384 searches in one batch, 32 threads per agent and
+queue capacity 16 (the shape the autotuner picks for this map), visited
+bitmap in global memory.  Checked through properties that do not depend on
+size: two runs agree bit for bit, a sample agrees with the oracle exactly,
+paths are connected chains of neighbours that end at their targets, and no
+path is shorter than the BFS optimum."""
+import numpy as np
+import pytest
+import torch
+
+from gmapf_b200 import path_quality as PQ
+from gmapf_b200 import scenarios as S
+from gpu_util import map_world, random_queries
+
+pytestmark = pytest.mark.gpu
+
+T, CAP, N_QUERIES, STRIDE = 32, 16, 16384, 16384
+
+
+def run(g, s, t):
+    n = len(s)
+    ds, dt = torch.from_numpy(s).cuda(), torch.from_numpy(t).cuda()
+    f = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ln = torch.zeros(n, dtype=torch.int32, device="cuda")
+    p = torch.full((n, STRIDE), -1, dtype=torch.int32, device="cuda")
+    st = g.search_batch_device(ds.data_ptr(), dt.data_ptr(), n, f.data_ptr(), ln.data_ptr(), p.data_ptr(), STRIDE)
+    torch.cuda.synchronize()
+    return f, ln, p, st
+
+
+def test_full_frame_batch(oracle_mod):
+    scn = S.cfg3(cells=160)
+    g = map_world(scn, T=T, Cap=CAP, visited_mode=3)
+    assert g.node_count > 100_000
+    s, t = random_queries(g, scn, N_QUERIES, seed=31)
+    f1, l1, p1, st1 = run(g, s, t)
+    f2, l2, p2, st2 = run(g, s, t)
+    assert torch.equal(f1, f2) and torch.equal(l1, l2) and torch.equal(p1, p2)
+    assert st1["rounds"] == st2["rounds"] and st1["expansions"] == st2["expansions"]
+    f, ln = f1.cpu().numpy(), l1.cpu().numpy()
+    assert f.sum() >= 0.99 * N_QUERIES  # the maze is connected; losses come only from bounded queues
+
+    rng = np.random.default_rng(32)
+    nodes = g.map_nodes()
+    # exact parity with the oracle on a sample (a search's result depends only
+    # on its own start and target, not on the rest of the batch)
+    idx = np.sort(rng.choice(N_QUERIES, 256, replace=False))
+    om = oracle_mod.OMap(nodes)
+    of, ol, op, _ = om.search_batch(s[idx], t[idx], T, CAP, scn.heuristic_k, path_stride=STRIDE)
+    sample = p1[torch.from_numpy(idx).cuda()].cpu().numpy()
+    assert np.array_equal(f[idx], of) and np.array_equal(ln[idx], ol)
+    for k in range(len(idx)):
+        if of[k]:
+            assert np.array_equal(sample[k, :ol[k]], op[k, :ol[k]]), f"query {idx[k]} differs from the oracle"
+
+    # connected chains of neighbours ending at the target (start excluded)
+    idx = np.sort(rng.choice(np.flatnonzero((f == 1) & (ln > 0)), 2048, replace=False))
+    rows = p1[torch.from_numpy(idx).cuda()].cpu().numpy()
+    nb = nodes["NeibsIdx"]
+    for k, i in enumerate(idx):
+        seq = np.concatenate([[s[i]], rows[k, :ln[i]]])
+        assert seq[-1] == t[i]
+        assert np.all((nb[seq[:-1]] == seq[1:, None]).any(axis=1)), f"query {i}: not a chain of neighbours"
+
+    # never shorter than the BFS optimum
+    idx = rng.choice(np.flatnonzero(f == 1), 128, replace=False)
+    hops, _ = PQ.optima(nodes, s[idx], t[idx])
+    assert np.all(ln[idx] >= hops)
