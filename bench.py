@@ -514,14 +514,20 @@ def bench_b200(args):
     all_queries = reduce_sum(dist, queries)
     value = all_queries / (dev_total_ms / 1e3)
 
+    # The extras below (path quality, many-frame percentiles, the Config-shape
+    # and plain forms, the CPU baseline, the multi-scene, serving and 64x64
+    # workloads) belong to the one-GPU line: a multi-GPU line carries the
+    # scaled metric only, so the GPUs of a scaling run are not held for them.
+    extras = ws == 1
+
     # path quality of the last device-timed frame (sample; outside the timing)
     quality = None
-    if rank == 0 and args.quality_sample > 0:
+    if extras and args.quality_sample > 0:
         quality = path_quality(g, args.quality_sample)
 
     # p99 over many full-retarget frames through the host API (fresh targets each)
     p99_long = None
-    if rank == 0 and args.p99_frames > 0:
+    if extras and args.p99_frames > 0:
         wl, _ = run_frames_host(g, target_sets(g, scn, rng, 3 + args.p99_frames, A), 3, args.p99_frames)
         p99_long = {"frames": args.p99_frames, "p50_step_ms": pct(wl, 50), "p99_step_ms": pct(wl, 99),
                     "max_step_ms": max(wl)}
@@ -547,7 +553,7 @@ def bench_b200(args):
 
     # batched form at the Config's own shape (same arithmetic as the plain form)
     fixed = None
-    if autotune and (Tb, Cb) != (T, C) and not args.no_plain:
+    if extras and autotune and (Tb, Cb) != (T, C) and not args.no_plain:
         scn_f, gf, rng_f = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A)
         msf, stf, _ = run_frames_device(gf, sets, W, K, torch, flush)
         fixed = {"threads_per_agent": T, "queue_capacity": C, "unit": "path queries/s",
@@ -558,7 +564,7 @@ def bench_b200(args):
 
     # plain per-agent form on the same frames
     plain = None
-    if not args.no_plain:
+    if extras and not args.no_plain:
         scn_p, gp, rng_p = make_scene(args.cells, seed, T, C, G.MODE_PLAIN, A)
         pk = max(2, min(K, 5))
         wall_p, pst = run_frames_host(gp, sets[:1 + pk], 1, pk)
@@ -567,22 +573,22 @@ def bench_b200(args):
         gp.close()
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if extras and not args.no_cpu:  # on rank 0 at N=1 only
         cpu = cpu_baseline(g, scn, sets, Tb, Cb, args.cpu_sample, os.cpu_count() or 1)
 
     # the multi-scene configuration (scene batch against separate contexts)
     multi = None
-    if rank == 0 and args.multi_scene_steps > 0:
+    if extras and args.multi_scene_steps > 0:
         multi = multi_scene(args.multi_scene_steps, 3)
 
     # the serving configuration (Poisson retargets, frames every 1/60 s)
     serve = None
-    if rank == 0 and args.serve_seconds > 0:
+    if extras and args.serve_seconds > 0:
         serve = serving([50000, 150000, 500000], args.serve_seconds)
 
     # secondary workload: the 64x64-cell maze of the configuration text
     secondary = None
-    if args.secondary_cells and args.secondary_cells != args.cells and rank == 0:
+    if extras and args.secondary_cells and args.secondary_cells != args.cells:
         scn2, g2, rng2 = make_scene(args.secondary_cells, 3, T, C, G.MODE_BATCHED, A, autotune=autotune)
         sh2 = g2.search_shape()
         sets2 = target_sets(g2, scn2, rng2, W + K, A)
