@@ -391,9 +391,13 @@ def serving(rates, duration_s: float, n_scenes: int = 8, agents: int = 8192):
 # --------------------------------------------------------------- b200 arm --
 
 def make_scene(cells, seed, T, C, mode, agents, profiler=True, autotune=False):
+    """The maze scene on this rank's GPU (LOCAL_RANK): the library context and
+    the device-resident targets the frames hand it share that device."""
+    import torch
     from gmapf_b200 import scenarios as S
     scn = S.cfg3(cells=cells, seed=seed, agents=agents, threads_per_agent=T, queue_capacity=C)
-    g, starts, rng = S.make_world(scn, mode=mode, profiler=profiler, autotune=autotune)
+    g, starts, rng = S.make_world(scn, mode=mode, profiler=profiler, autotune=autotune,
+                                  device=torch.cuda.current_device())
     t0 = time.perf_counter()
     g.ManualStart()  # device upload, landmarks and (batched) the autotuner
     g.startup_s = time.perf_counter() - t0
