@@ -502,6 +502,7 @@ int device_start(Context& c, std::string& err) {
 
 void device_free(Context& c) {
     Device& d = c.dev;
+    if (d.stream && cudaSetDevice(d.device) != cudaSuccess) cudaGetLastError();
     serve_free(c);
     if (d.stream) cudaStreamSynchronize(d.stream);
     if (d.stream2) cudaStreamSynchronize(d.stream2);

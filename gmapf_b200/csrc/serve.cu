@@ -535,6 +535,7 @@ int serve_submit(Context& c, const int* ids, const gmapf_v2* pos, int n, const i
 
 int serve_poll(Context& c, std::string& err) {
     Service& sv = *c.serve;
+    SCK(cudaSetDevice(c.dev.device));  // the context's GPU, whatever the caller's current one
     int rc = harvest(c, sv, err);
     if (rc) return rc;
     return admit_and_launch(c, sv, err);
@@ -622,6 +623,7 @@ int serve_drain(Context& c, double timeout_s, std::string& err) {
 int serve_result(Context& c, int agent, int* found, int* len, int* path, int cap, std::string& err) {
     // the agent's stashed result, not yet installed by a frame
     Service& sv = *c.serve;
+    SCK(cudaSetDevice(c.dev.device));
     if (!sv.to_install[agent]) {
         err = "no finished, uninstalled query for this agent";
         return GMAPF_E_STATE;
