@@ -204,6 +204,10 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device));
     size_t freeb = 0, totalb = 0;
     CK(cudaMemGetInfo(&freeb, &totalb));
+    // the search state this context already holds counts as free: a reshape
+    // reuses or replaces it
+    freeb += (size_t)d.rec_cap * (sizeof(Rec) * std::max(1, c.map.n) + sizeof(unsigned)) +
+             (size_t)d.gbm_cap * 4 * (size_t)d.bm_words;
     long long budget = c.opt.search_mem_budget > 0 ? c.opt.search_mem_budget : (40ll << 30);
     budget = std::min<long long>(budget, (long long)(freeb * 0.6));
     const long long per_slot = (long long)std::max(1, c.map.n) * (long long)sizeof(Rec);
@@ -255,30 +259,43 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     return GMAPF_OK;
 }
 
+void release(Context& c, void* p) {
+    if (!p) return;
+    Device& d = c.dev;
+    d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), p), d.allocs.end());
+    cudaFree(p);
+}
+
+// Search state for the shape in c (T, C, visited placement, block size).
+// The record and bitmap arrays are kept while the new shape's slots fit
+// them (the autotuner reshapes a hundred times; a ~12 GB free, allocation
+// and clear each time would take seconds).  Reuse needs no clearing: slot s
+// keeps its records together with its query epoch, so an old stamp never
+// equals a new epoch (modes 1 and 3 stamp 0, which no mode-2 epoch is), and
+// the bitmaps are cleared at the start of every query.
 int alloc_search_state(Context& c, std::string& err) {
     Device& d = c.dev;
     int blocks = 0;
     int rc = pick_slots(c, blocks, err);
     if (rc) return rc;
-    DALLOC(d.rec, (size_t)d.slots * std::max(1, c.map.n));
-    DALLOC(d.epoch, (size_t)d.slots);
-    if (d.vm == 3) DALLOC(d.gbm, (size_t)d.slots * d.bm_words);
-    return GMAPF_OK;
-}
-
-void free_search_state(Context& c) {
-    Device& d = c.dev;
-    for (void*& p : d.allocs) {
-        if (p == (void*)d.rec || p == (void*)d.epoch || (p && p == (void*)d.gbm)) {
-            cudaFree(p);
-            p = nullptr;
-        }
+    if (!d.rec || d.slots > d.rec_cap) {
+        release(c, d.rec);
+        release(c, d.epoch);
+        d.rec = nullptr;
+        d.epoch = nullptr;
+        d.rec_cap = 0;
+        DALLOC(d.rec, (size_t)d.slots * std::max(1, c.map.n));
+        DALLOC(d.epoch, (size_t)d.slots);
+        d.rec_cap = d.slots;
     }
-    d.allocs.erase(std::remove(d.allocs.begin(), d.allocs.end(), nullptr), d.allocs.end());
-    d.rec = nullptr;
-    d.epoch = nullptr;
-    d.gbm = nullptr;
-    d.slots = 0;
+    if (d.vm == 3 && (!d.gbm || d.slots > d.gbm_cap)) {
+        release(c, d.gbm);
+        d.gbm = nullptr;
+        d.gbm_cap = 0;
+        DALLOC(d.gbm, (size_t)d.slots * d.bm_words);
+        d.gbm_cap = d.slots;
+    }
+    return GMAPF_OK;
 }
 
 int search_blocks(Context& c) { return c.dev.slots / (c.block_threads / 32); }
@@ -510,6 +527,11 @@ void device_free(Context& c) {
     for (void* p : d.allocs)
         if (p) cudaFree(p);
     d.allocs.clear();
+    d.rec = nullptr;  // freed above: a later start allocates anew
+    d.epoch = nullptr;
+    d.gbm = nullptr;
+    d.rec_cap = d.gbm_cap = 0;
+    d.slots = 0;
     for (auto& e : d.ev)
         if (e) cudaEventDestroy(e), e = nullptr;
     if (d.frame_done) cudaEventDestroy(d.frame_done);
@@ -895,7 +917,6 @@ int device_debug_path(Context& c, int id, int* out, int cap, int* out_len, std::
 // Re-size the search state after the search parameters change (autotuner).
 int device_reconfigure_search(Context& c, std::string& err) {
     destroy_graph(c);
-    free_search_state(c);
     return alloc_search_state(c, err);
 }
 
@@ -989,18 +1010,24 @@ int device_autotune(Context& c, std::string& err) {
     // already below the best found count skips its other placements.
     std::vector<int> Ts = {32, 16, 8, 4, 2}, Cs = {8, 16, 32, 64, 128, 256};  // likely-fast shapes first
     if (std::find(Cs.begin(), Cs.end(), C0) == Cs.end()) Cs.push_back(C0);
+    // Fewer threads per agent mean more rounds per query: once the best time
+    // at one T is over twice the best so far, the smaller T are not tried.
     long long best_found_so_far = 0;
-    for (int T : Ts)
+    for (int T : Ts) {
+        float best_at_T = 1e30f;
         for (int C : Cs)
             for (int vm : {3, 2, 1}) {
                 if (c.opt.visited_mode != 0 && c.opt.visited_mode != vm) continue;
                 const size_t before = trials.size();
                 trial(T, C, vm, 0);
                 if (trials.size() == before) continue;  // shape does not fit this placement
+                best_at_T = std::min(best_at_T, trials.back().ms);
                 const long long f = trials.back().found;
                 best_found_so_far = std::max(best_found_so_far, f);
                 if ((double)f < (double)best_found_so_far * 0.999) break;
             }
+        if (best_at_T < 1e30f && best_at_T > 2.0f * best_so_far) break;
+    }
     auto choose = [&]() -> const Trial* {
         long long best_found = 0;
         for (const Trial& t : trials) best_found = std::max(best_found, t.found);

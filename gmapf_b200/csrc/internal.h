@@ -255,6 +255,7 @@ struct Device {
     int vm = 2;                 // visited mode (1, 2 or 3; see launch_search)
     unsigned* gbm = nullptr;    // visited mode 3: slots x bm_words
     int bm_words = 0;           // bitmap words per slot
+    int rec_cap = 0, gbm_cap = 0;  // slots the record / bitmap arrays hold (kept across reshapes)
     // agent grid
     int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
         *cell_items = nullptr;
