@@ -76,6 +76,18 @@ def test_cfg2_retargets(oracle_mod, vm):
     run(g, ow, scn, 250, rng, retarget_every=100, check_every=25)
 
 
+@pytest.mark.parametrize("vm", [2, 3])
+def test_cfg2_full_run(oracle_mod, vm):
+    # the configuration as specified: 2,048 agents on the 1000x1000 map with
+    # 200 rectangles, every agent retargeted every 100 steps, 1,000 steps
+    scn = S.cfg2()
+    g, ow, rng = make_pair(oracle_mod, scn, 2048, vm=vm)
+    d = run(g, ow, scn, 1000, rng, retarget_every=100, check_every=50)
+    for i in range(0, 2048, 97):
+        if d["path_len"][i] > 0:
+            assert np.array_equal(g.path(i), ow.path(i))
+
+
 def test_plain_mode_step(oracle_mod):
     scn = S.cfg1()
     g, ow, rng = make_pair(oracle_mod, scn, 128, mode=G.MODE_PLAIN)
