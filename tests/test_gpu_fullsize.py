@@ -4,7 +4,10 @@ queue capacity 16 (the shape the autotuner picks for this map), visited
 bitmap in global memory.  Checked through properties that do not depend on
 size: two runs agree bit for bit, a sample agrees with the oracle exactly,
 paths are connected chains of neighbours that end at their targets, and no
-path is shorter than the BFS optimum."""
+path is shorter than the BFS optimum.  The per-frame step at the same size
+(16,384 agents) is compared with the oracle world frame by frame."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -12,6 +15,7 @@ import torch
 from gmapf_b200 import path_quality as PQ
 from gmapf_b200 import scenarios as S
 from gpu_util import map_world, random_queries
+from test_gpu_step import make_pair, retarget, run as run_steps
 
 pytestmark = pytest.mark.gpu
 
@@ -67,3 +71,19 @@ def test_full_frame_batch(oracle_mod):
     idx = rng.choice(np.flatnonzero(f == 1), 128, replace=False)
     hops, _ = PQ.optima(nodes, s[idx], t[idx])
     assert np.all(ln[idx] >= hops)
+
+
+def test_full_frame_steps(oracle_mod):
+    # the step itself at this size: 16,384 agents all retargeted in one frame
+    # (compaction, search, path rows), then two frames of movement and
+    # collisions, each compared with the oracle world (states, nodes, path
+    # steps exactly; positions within 1e-4 relative)
+    scn = S.cfg3(cells=160)
+    A = 16384
+    g, ow, rng = make_pair(oracle_mod, scn, A, T=T, Cap=CAP, vm=3)
+    retarget(g, ow, scn, np.arange(A), rng)
+    d = run_steps(g, ow, scn, 3, rng, check_every=1, threads=os.cpu_count() or 8)
+    assert (d["path_len"] > 0).sum() >= 0.99 * A
+    for i in range(0, A, 509):
+        if d["path_len"][i] > 0:
+            assert np.array_equal(g.path(i), ow.path(i))
