@@ -93,6 +93,17 @@ def test_batch_matches_scenes_alone(oracle_mod, vm):
     batch.close()
 
 
+def test_cfg4_full_run(oracle_mod):
+    # the configuration as specified: 64 scenes (sides 200..2000, 10..500
+    # rectangles, 64..1024 agents of radius 1..3), retargets with probability
+    # 0.02 per agent per step, 500 steps, one scene batch
+    scns = S.cfg4()
+    scenes, worlds, rngs = build(oracle_mod, scns)
+    batch = G.SceneBatch(scenes)
+    run(scns, scenes, worlds, rngs, batch, 500, check_every=50)
+    batch.close()
+
+
 def test_batch_per_scene_request_limits(oracle_mod):
     # PathFinderParallelAgents below the agent count: each scene defers its own overflow
     scns = S.cfg4(4, seed=10, agents_range=(60, 120))
