@@ -173,3 +173,41 @@ def test_scene_batch_serving(oracle_mod):
             res.append((f, L, p - nb0))
         oracle_check(oracle_mod, g, 8, 32, g.locate(pos[ids]), g.locate(tp), res)
     b.close()
+
+
+def test_serving_configuration_scale(oracle_mod):
+    # the serving configuration's size: 8 resident scenes of the 1000x1000,
+    # 200-rectangle type with 8,192 agents each (one scene batch), 32,768
+    # retargets submitted in one burst and drained; a sample of the results
+    # against the oracle
+    scns = [S.cfg2(seed=21 + k) for k in range(8)]
+    scenes = []
+    for scn in scns:
+        g = G.GMAPF()
+        g.Init(G.make_config(8192, scn.radius, scn.speed, 8192, 8, 32, scn.heuristic_k))
+        S.build_map(g, scn)
+        for p in S.free_points(g, scn, 8192, np.random.default_rng(scn.seed)):
+            g.AddAgent(p)
+        scenes.append(g)
+    b = G.SceneBatch(scenes)
+    b.world.serve_start()
+    subs = []
+    for s, (scn, g) in enumerate(zip(scns, scenes)):
+        rng = np.random.default_rng(300 + s)
+        ids = np.sort(rng.choice(8192, 4096, replace=False)).astype(np.int32)
+        tp = S.free_points(g, scn, len(ids), rng)
+        g.serve_submit(ids, tp)
+        subs.append((ids, tp))
+    b.world.serve_drain()
+    st = b.world.serve_stats()
+    assert st["completed"] == 8 * 4096 and st["in_flight"] == 0 and st["waiting"] == 0
+    for s, (g, (ids, tp)) in enumerate(zip(scenes, subs)):
+        ab, nb0 = b.scene_base(s)
+        pos, _ = g.agents()
+        pick = np.arange(0, len(ids), 64)
+        res = []
+        for k in pick:
+            f, L, p = b.world.serve_result(int(ids[k]) + ab)
+            res.append((f, L, p - nb0))
+        oracle_check(oracle_mod, g, 8, 32, g.locate(pos[ids[pick]]), g.locate(tp[pick]), res)
+    b.close()
