@@ -130,6 +130,7 @@ SIGNATURES = {
     "gmapf_search_shape": (C.c_int, [P, I32P, I32P, I32P, I32P, I32P]),
     "gmapf_set_tune_cache": (C.c_int, [P, C.c_char_p]),
     "gmapf_tune_source": (C.c_int, [P, I32P]),
+    "gmapf_set_search_timeline": (C.c_int, [P, C.c_void_p, C.c_int32]),
     "gmapf_stream_handle": (C.c_void_p, [P]),
     "gmapf_search_batch_host": (C.c_int, [P, I32P, I32P, C.c_int32, I32P, I32P, I32P, C.c_int32,
                                           C.POINTER(StepStats)]),

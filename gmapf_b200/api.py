@@ -316,6 +316,11 @@ class GMAPF:
         """Autotuner cache file (before the start); None turns it off."""
         self._check(self._lib.gmapf_set_tune_cache(self._h, None if path is None else str(path).encode()))
 
+    def set_search_timeline(self, d_timeline: int, rows: int) -> None:
+        """Device buffer (raw address) of 2 x rows uint64 for the batch searches'
+        per-request start and end times (GPU global timer, ns); 0 turns it off."""
+        self._check(self._lib.gmapf_set_search_timeline(self._h, d_timeline or None, int(rows)))
+
     def tune_source(self) -> int:
         """0: the Config's shape, 1: tuned at the start, 2: from the autotuner cache."""
         v = C.c_int32()

@@ -830,6 +830,15 @@ gmapf_status gmapf_set_tune_cache(gmapf_ctx* ctx, const char* path) {
     return GMAPF_OK;
 }
 
+gmapf_status gmapf_set_search_timeline(gmapf_ctx* ctx, uint64_t* d_timeline, int32_t rows) {
+    NEED_CTX(ctx);
+    if (ctx->world || ctx->c.detached) return scene_only("search timeline");
+    if (d_timeline && rows <= 0) return fail(GMAPF_E_INVALID_ARG, "timeline rows must be positive");
+    ctx->c.timeline = reinterpret_cast<unsigned long long*>(d_timeline);
+    ctx->c.timeline_rows = d_timeline ? rows : 0;
+    return GMAPF_OK;
+}
+
 gmapf_status gmapf_tune_source(gmapf_ctx* ctx, int32_t* source) {
     NEED_CTX(ctx);
     if (!source) return fail(GMAPF_E_INVALID_ARG, "null output pointer");

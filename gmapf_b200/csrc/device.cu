@@ -819,6 +819,14 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
     sp.ag_state = nullptr;
     sp.ag_step_idx = nullptr;
     sp.ag_path_len = nullptr;
+    if (c.timeline) {
+        if (n > c.timeline_rows) {
+            err = "the search timeline holds " + std::to_string(c.timeline_rows) + " requests, the batch has " +
+                  std::to_string(n);
+            return GMAPF_E_INVALID_ARG;
+        }
+        sp.timeline = c.timeline;
+    }
     CK(cudaEventRecord(d.ev[6], s));
     if (n > 0) {
         if (c.opt.mode == GMAPF_MODE_BATCHED) {

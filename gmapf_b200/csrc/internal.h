@@ -81,6 +81,10 @@ struct SearchParams {
     int ring_cap;
     int ring_base;
     unsigned long long* done;
+    // diagnostics (batch searches): per output row, the GPU global timer when
+    // a warp took the request [2 row] and when its results were written
+    // [2 row + 1], or null
+    unsigned long long* timeline;
 };
 
 // Per-scene constants of the mover and of point location: one entry for a
@@ -338,6 +342,8 @@ struct Context {
     // autotuner's choices where the options leave them open (0: pick by occupancy)
     int tuned_vm = 0, tuned_bt = 0;
     std::string tune_cache;  // autotuner cache file ("" = none)
+    unsigned long long* timeline = nullptr;  // caller's device buffer (gmapf_set_search_timeline)
+    int timeline_rows = 0;
     int tune_source = 0;     // 0 not tuned, 1 tuned at the start, 2 from the cache
     // device
     Device dev;

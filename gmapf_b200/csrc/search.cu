@@ -127,6 +127,12 @@ __device__ __forceinline__ void bm_set(unsigned* bm, int n, int dir) {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Serving ring: publish query q's completion after its results (lane 0,
 // after the warp's writes are ordered by __syncwarp)
 __device__ __forceinline__ void ring_complete(const SearchParams& p, int slot_row, int q, int found) {
@@ -202,6 +208,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
         if (start < 0 || start >= n_nodes || target < 0 || target >= n_nodes || start == target) {
             const bool bad = start != target || start < 0 || start >= n_nodes;
             if (lane == 0) {  // bad request: not found; start == target: found, empty path
+                if (p.timeline) p.timeline[2 * (long long)orow] = p.timeline[2 * (long long)orow + 1] = global_timer_ns();
                 if (bad) atomicOr(p.err, ERR_BAD_REQUEST);
                 if (p.out_found) p.out_found[orow] = bad ? 0 : 1;
                 if (p.out_len) p.out_len[orow] = 0;
@@ -215,6 +222,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             continue;
         }
 
+        if (p.timeline && lane == 0) p.timeline[2 * (long long)orow] = global_timer_ns();
         unsigned ep = 0;
         if (VM == 2) {
             unsigned e = 0;
@@ -578,6 +586,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             atomicAdd(p.stats + ST_PATH_NODES, (unsigned long long)L);
             atomicAdd(p.stats + ST_FOUND, (unsigned long long)found);
             if (p.done) ring_complete(p, orow, p.ring_base + r, found);
+            if (p.timeline) p.timeline[2 * (long long)orow + 1] = global_timer_ns();
         }
     }
 }

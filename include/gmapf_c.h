@@ -228,6 +228,13 @@ gmapf_status gmapf_search_shape(gmapf_ctx* ctx, int32_t* T, int32_t* C, int32_t*
  * Set before the start; NULL or "" turns it off.  A file that cannot be read
  * or written only costs the time of tuning. */
 gmapf_status gmapf_set_tune_cache(gmapf_ctx* ctx, const char* path);
+/* Search timeline (diagnostics, no reference counterpart): with a device
+ * buffer of 2 x rows uint64 set, each later gmapf_search_batch_host/_device
+ * call of at most `rows` requests writes for request i the GPU global timer
+ * (ns) when a warp took it, at [2i], and when its results were written, at
+ * [2i + 1].  A larger batch is rejected (GMAPF_E_INVALID_ARG).  NULL turns it
+ * off.  Frames are not recorded. */
+gmapf_status gmapf_set_search_timeline(gmapf_ctx* ctx, uint64_t* d_timeline, int32_t rows);
 /* how the started context's search shape was chosen: 0 the Config's (no
  * autotune), 1 tuned at the start, 2 taken from the autotuner cache */
 gmapf_status gmapf_tune_source(gmapf_ctx* ctx, int32_t* source);

@@ -154,6 +154,15 @@ def test_tune_cache_is_set_before_the_start(tmp_path):
     assert e.value.status_name == "GMAPF_E_STATE"
 
 
+def test_search_timeline_arguments():
+    scn = S.cfg1()
+    g, starts, rng = S.make_world(scn, agents=4)
+    with pytest.raises(G.GMAPFError) as e:
+        g.set_search_timeline(0x1000, 0)  # a buffer needs a positive row count
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
+    g.set_search_timeline(0, 0)
+
+
 def test_bulk_retarget_stops_at_the_first_invalid_point():
     # large bulks locate in parallel; the items before the first invalid one
     # are applied, the rest are not (as one call per item would do)

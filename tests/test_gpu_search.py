@@ -136,6 +136,26 @@ def test_autotune_cache_reuses_the_shape(oracle_mod, tmp_path):
     assert len(path.read_text().splitlines()) == 3
 
 
+def test_search_timeline():
+    import torch
+    scn = S.cfg3(cells=32)
+    g = map_world(scn, T=8, Cap=16)
+    s, t = random_queries(g, scn, 1000, seed=40)
+    a = g.search_batch(s, t, g.node_count)
+    buf = torch.zeros(2 * 1000, dtype=torch.int64, device="cuda")
+    g.set_search_timeline(buf.data_ptr(), 1000)
+    b = g.search_batch(s, t, g.node_count)  # recording changes no result
+    assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
+    tl = buf.cpu().numpy().reshape(-1, 2)
+    assert np.all(tl[:, 0] > 0) and np.all(tl[:, 1] >= tl[:, 0])
+    s2, t2 = np.concatenate([s, s]), np.concatenate([t, t])
+    with pytest.raises(G.GMAPFError) as e:  # more requests than the buffer holds
+        g.search_batch(s2, t2, g.node_count)
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
+    g.set_search_timeline(0, 0)
+    g.search_batch(s2, t2, g.node_count)
+
+
 def test_longest_first_order_does_not_change_results(oracle_mod):
     scn = S.cfg3(cells=32)
     go = map_world(scn, T=8, Cap=16, order=True)
