@@ -37,8 +37,10 @@
 //     32-byte records themselves, stamped with the query epoch (no clearing
 //     between queries, but one DRAM round trip per round);
 //   - records (G, parent and five further ancestors) are written once per
-//     claimed node; the path walk reads one record per six hops; a node's
-//     record is read when it is expanded, in flight together with its row;
+//     claimed node, each as one 32-byte access; the path walk reads one
+//     record per six hops; a node's record is read when it is expanded, in
+//     flight together with its row (T <= 8) or with its neighbours' visited
+//     state (T >= 16);
 //   - idle warps refill from a device work counter (persistent form) or
 //     stop (plain form).
 #include <cuda_runtime.h>
