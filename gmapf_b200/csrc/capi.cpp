@@ -44,6 +44,18 @@ gmapf_status fail(int code, const std::string& msg) {
     if ((ctx)->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");   \
     gmapf_ctx* w = (ctx)->world
 
+// A pointer a kernel may be given: device, managed or mapped host memory.
+// Pageable host memory (the usual mistake with the *_device entry points)
+// is refused before anything is launched, instead of faulting the GPU.
+bool gpu_reachable(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type != cudaMemoryTypeUnregistered;
+}
+
 gmapf_status scene_only(const char* what) {
     return fail(GMAPF_E_STATE, std::string(what) + ": this scene is stepped by its batch (use the batch's world)");
 }
@@ -583,6 +595,8 @@ gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_id
     if (!c.started) return fail(GMAPF_E_STATE, "not started");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
     if (n < 0 || (n > 0 && (!d_ids || !d_pos))) return fail(GMAPF_E_INVALID_ARG, "bad device arrays");
+    if (n > 0 && !(gpu_reachable(d_ids) && gpu_reachable(d_pos)))
+        return fail(GMAPF_E_INVALID_ARG, "a buffer is not GPU memory (device, managed or mapped pinned)");
     if (n == 0) return GMAPF_OK;
     std::string err;
     int rc = device_set_targets_device(c, d_ids, d_pos, n, id_base, id_count, err);
@@ -834,6 +848,8 @@ gmapf_status gmapf_set_search_timeline(gmapf_ctx* ctx, uint64_t* d_timeline, int
     NEED_CTX(ctx);
     if (ctx->world || ctx->c.detached) return scene_only("search timeline");
     if (d_timeline && rows <= 0) return fail(GMAPF_E_INVALID_ARG, "timeline rows must be positive");
+    if (d_timeline && !gpu_reachable(d_timeline))
+        return fail(GMAPF_E_INVALID_ARG, "the timeline is not GPU memory (device, managed or mapped pinned)");
     ctx->c.timeline = reinterpret_cast<unsigned long long*>(d_timeline);
     ctx->c.timeline_rows = d_timeline ? rows : 0;
     return GMAPF_OK;
@@ -874,6 +890,9 @@ gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, 
     if (n < 0 || path_stride < 1) return fail(GMAPF_E_INVALID_ARG, "bad sizes");
     if (n > 0 && (!d_starts || !d_targets || !d_found || !d_lens || !d_paths))
         return fail(GMAPF_E_INVALID_ARG, "null device pointer");
+    if (n > 0 && !(gpu_reachable(d_starts) && gpu_reachable(d_targets) && gpu_reachable(d_found) &&
+                   gpu_reachable(d_lens) && gpu_reachable(d_paths)))
+        return fail(GMAPF_E_INVALID_ARG, "a buffer is not GPU memory (device, managed or mapped pinned)");
     gmapf_status s = start_if_needed(c);
     if (s != GMAPF_OK) return s;
     std::string err;

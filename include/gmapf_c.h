@@ -165,7 +165,8 @@ gmapf_status gmapf_set_agent_targ_pos_bulk(gmapf_ctx* ctx, const int32_t* ids, c
  * target triangles are located on the device (same rule as the host path).
  * Enqueued on the context's stream before the next step; a position in no
  * triangle leaves that agent unchanged and makes the next step report
- * GMAPF_E_DEVICE.  Call after the start, not during a step. */
+ * GMAPF_E_DEVICE.  Call after the start, not during a step.  Pageable host
+ * memory is refused (GMAPF_E_INVALID_ARG). */
 gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_ids, const gmapf_v2* d_pos, int32_t n);
 
 /* GMAPF::ManualStart()                   -- src/GMAPF.cu:72-130 */
@@ -248,7 +249,9 @@ gmapf_status gmapf_search_batch_host(gmapf_ctx* ctx, const int32_t* starts, cons
                                      int32_t n, int32_t* found, int32_t* lens, int32_t* paths,
                                      int32_t path_stride, gmapf_step_stats* stats);
 /* Same with device pointers already resident in HBM (no copies); ordered
- * on the context's stream; synchronous. */
+ * on the context's stream; synchronous.  Buffers must be GPU memory
+ * (device, managed or mapped pinned); pageable host memory is refused with
+ * GMAPF_E_INVALID_ARG before anything runs. */
 gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, const int32_t* d_targets,
                                        int32_t n, int32_t* d_found, int32_t* d_lens, int32_t* d_paths,
                                        int32_t path_stride, gmapf_step_stats* stats);

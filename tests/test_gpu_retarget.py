@@ -73,3 +73,17 @@ def test_bulk_retarget_while_a_step_runs():
     g.WaitStepEnd()
     d = g.debug_agents()
     assert np.array_equal(d["targ_node"], g.locate(tp))
+
+
+def test_device_retarget_refuses_host_memory():
+    scn = S.cfg2()
+    g, starts, rng = S.make_world(scn, agents=64)
+    g.ManualStart()
+    ids = np.arange(64, dtype=np.int32)
+    tp = S.free_points(g, scn, 64, rng).astype(np.float32)
+    with pytest.raises(G.GMAPFError) as e:
+        g.set_targets_device(ids.ctypes.data, tp.ctypes.data, 64)
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
+    g.AsyncStep(scn.dt)  # nothing was applied; the context steps on
+    g.WaitStepEnd()
+    assert np.all(g.debug_agents()["state"] == int(G.EAgentState.Idle))

@@ -156,6 +156,26 @@ def test_search_timeline():
     g.search_batch(s2, t2, g.node_count)
 
 
+def test_device_entry_points_refuse_host_memory():
+    # pageable host buffers handed to the *_device entry points are refused
+    # before any launch (GMAPF_E_INVALID_ARG), not read by a kernel
+    scn = S.cfg2()
+    g = map_world(scn, T=8, Cap=32)
+    s, t = random_queries(g, scn, 64, seed=41)
+    found, lens = np.zeros(64, np.int32), np.zeros(64, np.int32)
+    paths = np.zeros((64, 8), np.int32)
+    with pytest.raises(G.GMAPFError) as e:
+        g.search_batch_device(s.ctypes.data, t.ctypes.data, 64, found.ctypes.data, lens.ctypes.data,
+                              paths.ctypes.data, 8)
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
+    tl = np.zeros(128, np.uint64)
+    with pytest.raises(G.GMAPFError) as e:
+        g.set_search_timeline(tl.ctypes.data, 64)
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
+    f, ln, p, st = g.search_batch(s, t, g.node_count)  # the context is unharmed
+    assert st["requests"] == 64
+
+
 def test_longest_first_order_does_not_change_results(oracle_mod):
     scn = S.cfg3(cells=32)
     go = map_world(scn, T=8, Cap=16, order=True)
