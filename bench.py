@@ -710,6 +710,67 @@ def bench_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------- profiling runs --
+
+def timeline_summary(tl: np.ndarray, slots: int) -> dict:
+    """tl: (n, 2) start/end in ns of one batch; times in ms from the first start."""
+    t0 = int(tl[:, 0].min())
+    st = (tl[:, 0].astype(np.int64) - t0) / 1e6
+    en = (tl[:, 1].astype(np.int64) - t0) / 1e6
+    total = float(en.max())
+    grid = np.linspace(0.0, total, 11)
+    active = [int(((st <= x) & (en > x)).sum()) for x in grid]
+    # the first moment after the ramp at which fewer than 90% of the slots are busy
+    busy = [x for x, a in zip(grid, active) if x > 0 and a < 0.9 * min(slots, len(tl))]
+    dur = en - st
+    i = int(np.argmax(dur))
+    return {"launch_ms": round(total, 3),
+            "all_slots_busy_until_ms": round(float(busy[0]), 3) if busy else round(total, 3),
+            "last_start_ms": round(float(st.max()), 3),
+            "done_90_99_ms": [round(float(np.percentile(en, q)), 3) for q in (90, 99)],
+            "slowest": {"request": i, "start_ms": round(float(st[i]), 3), "ms": round(float(dur[i]), 3)},
+            "running_at": [[round(float(x), 2), a] for x, a in zip(grid, active)]}
+
+
+def profile_search(spec: str, budget_mb: int, timeline: bool):
+    """One batch search on a seeded maze, for profilers (ncu -k k_search):
+    spec = "CELLS,T,C,VISITED_MODE,QUERIES".  Builds the CELLS x CELLS maze of
+    the batched-uneven-queries configuration, draws QUERIES seeded free-space
+    start/target pairs (numpy default_rng(7), starts then targets) and runs
+    gmapf_search_batch_host once with threads per agent T, queue capacity C
+    and visited mode 1 (shared-memory bitmap), 2 (global records) or 3
+    (global bitmap); budget_mb caps the search state (and so the resident
+    slots) to keep a capture small.  Paths are not kept (2-entry rows: long
+    paths raise the path-capacity flag, which is expected).  With timeline,
+    each request's start and end on the GPU global timer are recorded
+    (gmapf_set_search_timeline) and summarised."""
+    import gmapf_b200 as G
+    from gmapf_b200 import scenarios as S
+    cells, T, C, vm, nq = (int(x) for x in spec.split(","))
+    scn = S.cfg3(cells=cells)
+    g = G.GMAPF()
+    g.Init(G.make_config(4, scn.radius, scn.speed, 4, T, C, scn.heuristic_k))
+    g.set_options(visited_mode=vm, search_mem_budget=budget_mb << 20)
+    S.build_map(g, scn)
+    rng = np.random.default_rng(7)
+    s = g.locate(S.free_points(g, scn, nq, rng)).astype(np.int32)
+    t = g.locate(S.free_points(g, scn, nq, rng)).astype(np.int32)
+    buf = None
+    if timeline:
+        import torch
+        buf = torch.zeros(2 * nq, dtype=torch.int64, device="cuda")
+        g.set_search_timeline(buf.data_ptr(), nq)
+    try:
+        g.search_batch(s, t, 2)
+    except G.GMAPFError:
+        pass
+    out = {"search_ms": g.last_search_ms(), "shape": g.search_shape()}
+    if timeline:
+        out["timeline"] = timeline_summary(buf.cpu().numpy().reshape(nq, 2), g.search_shape()["slots"])
+    print(json.dumps(out), flush=True)
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -733,7 +794,14 @@ def main():
     ap.add_argument("--quality-sample", type=int, default=128, help="agents whose paths are compared with BFS/Dijkstra")
     ap.add_argument("--no-autotune", action="store_true", help="batched form at the Config's T and C")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-search", default="", metavar="CELLS,T,C,VM,QUERIES",
+                    help="profiling run: one batch search on the CELLS maze (no bench line)")
+    ap.add_argument("--profile-budget-mb", type=int, default=0, help="search-state cap of --profile-search")
+    ap.add_argument("--profile-timeline", action="store_true", help="--profile-search: per-request timeline")
     args = ap.parse_args()
+    if args.profile_search:
+        profile_search(args.profile_search, args.profile_budget_mb, args.profile_timeline)
+        return
     if args.warmup < 3:
         log("warmup raised to 3 (timing rule)")
         args.warmup = 3

@@ -51,7 +51,8 @@ class Options(C.Structure):
         ("order_by_estimate", C.c_int32),
         ("visited_mode", C.c_int32),
         ("path_smoothing", C.c_int32),
-        ("_reserved", C.c_int32 * 3),
+        ("round_limit", C.c_int32),
+        ("_reserved", C.c_int32 * 2),
     ]
 
 
@@ -74,7 +75,7 @@ class StepStats(C.Structure):
         ("rounds", C.c_int64), ("deg_sum", C.c_int64), ("claims", C.c_int64),
         ("path_nodes", C.c_int64), ("moving", C.c_int64),
         ("ms_step_wall", C.c_float), ("ms_search", C.c_float), ("ms_mover", C.c_float),
-        ("ms_total_device", C.c_float),
+        ("ms_total_device", C.c_float), ("neighbours", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -154,8 +155,8 @@ SIGNATURES = {
     "gmapf_batch_world": (P, [P]),
     "gmapf_batch_scene_base": (C.c_int, [P, C.c_int32, I32P, I32P]),
     "gmapf_search_batch_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
-                                             C.c_int32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
-                                             C.c_void_p]),
+                                             C.c_int32, C.c_float, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_int32, C.c_void_p]),
 }
 
 _lib = None

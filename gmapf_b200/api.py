@@ -61,8 +61,9 @@ def make_config(agents_max: int, radius: float, speed: float, parallel_agents: i
 
 def make_options(mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0, autotune: bool = False,
                  search_mem_budget: int = 0, order_by_estimate: bool = True, visited_mode: int = 0,
-                 path_smoothing: bool = False) -> Options:
+                 path_smoothing: bool = False, round_limit: int = 0) -> Options:
     o = Options()
+    o.round_limit = round_limit
     o.path_smoothing = 1 if path_smoothing else 0
     o.device = device
     o.mode = mode
@@ -188,7 +189,8 @@ class GMAPF:
     # -- extras ------------------------------------------------------------
     def set_options(self, **kw) -> None:
         """mode, device, block_threads, autotune, search_mem_budget,
-        order_by_estimate, visited_mode (see gmapf_options)."""
+        order_by_estimate, visited_mode, path_smoothing, round_limit (see
+        gmapf_options)."""
         o = make_options(**kw)
         self._check(self._lib.gmapf_set_options(self._h, C.byref(o)))
 

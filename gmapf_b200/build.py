@@ -34,11 +34,15 @@ CPP_SOURCES = ["hostmap.cpp", "capi.cpp"]
 CDT_SOURCE = "navmesh_cdt.cpp"
 
 
+# Where the reference project's source tree lies (build time only: its CDT
+# headers are compiled into the navmesh builder, and its container headers
+# into the oracle's pinning harness).  Nothing at run time reads it.
+REF_DIR = os.environ.get("GMAPF_REF_DIR", "/root/reference")
+
+
 def cdt_dir() -> str | None:
-    d = os.environ.get("GMAPF_CDT_DIR")
-    if d is None:
-        d = "/root/reference/include"
-    if d and os.path.isfile(os.path.join(d, "CDT", "CDT.h")):
+    d = os.environ.get("GMAPF_CDT_DIR") or os.path.join(REF_DIR, "include")
+    if os.path.isfile(os.path.join(d, "CDT", "CDT.h")):
         return d
     return None
 
@@ -95,9 +99,11 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
 
 def build_oracle(force: bool = False) -> Path:
     out = ORACLE_DIR / "liboracle.so"
-    deps = [ORACLE_DIR / "gmapf_oracle.cpp", ORACLE_DIR / "gmapf_oracle.h", ORACLE_DIR / "Makefile"]
+    deps = [ORACLE_DIR / "gmapf_oracle.cpp", ORACLE_DIR / "gmapf_oracle.h", ORACLE_DIR / "navmesh_oracle.cpp",
+            ORACLE_DIR / "Makefile"]
     if force or needs_build(out, deps):
-        _run(["make", "-s", "-C", str(ORACLE_DIR), "-B" if force else "all"])
+        cdt = cdt_dir()
+        _run(["make", "-s", "-C", str(ORACLE_DIR), "-B" if force else "all"] + ([f"CDT_DIR={cdt}"] if cdt else []))
     return out
 
 

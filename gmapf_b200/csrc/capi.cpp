@@ -13,6 +13,25 @@
 
 using namespace gmapf_b200;
 
+namespace gmapf_b200 {
+
+// A pointer a kernel on `device` may be given: device memory of that GPU,
+// managed memory or mapped host memory.  Pageable host memory (the usual
+// mistake with the *_device entry points) and device memory of another GPU
+// are refused before anything is launched, instead of faulting the GPU.
+bool gpu_reachable(const void* p, int device) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeUnregistered) return false;
+    if (a.type == cudaMemoryTypeDevice && a.device != device) return false;
+    return true;
+}
+
+}  // namespace gmapf_b200
+
 struct gmapf_batch;
 
 struct gmapf_ctx {
@@ -43,18 +62,6 @@ gmapf_status fail(int code, const std::string& msg) {
 #define SCENE_WORLD(ctx, w)                                                                  \
     if ((ctx)->c.detached) return fail(GMAPF_E_STATE, "the scene's batch was destroyed");   \
     gmapf_ctx* w = (ctx)->world
-
-// A pointer a kernel may be given: device, managed or mapped host memory.
-// Pageable host memory (the usual mistake with the *_device entry points)
-// is refused before anything is launched, instead of faulting the GPU.
-bool gpu_reachable(const void* p) {
-    cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type != cudaMemoryTypeUnregistered;
-}
 
 gmapf_status scene_only(const char* what) {
     return fail(GMAPF_E_STATE, std::string(what) + ": this scene is stepped by its batch (use the batch's world)");
@@ -193,6 +200,7 @@ gmapf_status gmapf_set_options(gmapf_ctx* ctx, const gmapf_options* o) {
     if (o->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
     if (o->visited_mode < 0 || o->visited_mode > 3)
         return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
+    if (o->round_limit < 0) return fail(GMAPF_E_INVALID_ARG, "round_limit must be >= 0 (0: no practical limit)");
     c.opt = *o;
     if (o->block_threads) c.block_threads = o->block_threads;
     return GMAPF_OK;
@@ -595,8 +603,8 @@ gmapf_status gmapf_set_agent_targ_pos_device(gmapf_ctx* ctx, const int32_t* d_id
     if (!c.started) return fail(GMAPF_E_STATE, "not started");
     if (c.step_going) return fail(GMAPF_E_STATE, "a step is running");
     if (n < 0 || (n > 0 && (!d_ids || !d_pos))) return fail(GMAPF_E_INVALID_ARG, "bad device arrays");
-    if (n > 0 && !(gpu_reachable(d_ids) && gpu_reachable(d_pos)))
-        return fail(GMAPF_E_INVALID_ARG, "a buffer is not GPU memory (device, managed or mapped pinned)");
+    if (n > 0 && !(gpu_reachable(d_ids, c.opt.device) && gpu_reachable(d_pos, c.opt.device)))
+        return fail(GMAPF_E_INVALID_ARG, "a buffer is not memory the context's GPU can reach (its device memory, managed or mapped pinned)");
     if (n == 0) return GMAPF_OK;
     std::string err;
     int rc = device_set_targets_device(c, d_ids, d_pos, n, id_base, id_count, err);
@@ -848,8 +856,8 @@ gmapf_status gmapf_set_search_timeline(gmapf_ctx* ctx, uint64_t* d_timeline, int
     NEED_CTX(ctx);
     if (ctx->world || ctx->c.detached) return scene_only("search timeline");
     if (d_timeline && rows <= 0) return fail(GMAPF_E_INVALID_ARG, "timeline rows must be positive");
-    if (d_timeline && !gpu_reachable(d_timeline))
-        return fail(GMAPF_E_INVALID_ARG, "the timeline is not GPU memory (device, managed or mapped pinned)");
+    if (d_timeline && !gpu_reachable(d_timeline, ctx->c.opt.device))
+        return fail(GMAPF_E_INVALID_ARG, "the timeline is not memory the context's GPU can reach (its device memory, managed or mapped pinned)");
     ctx->c.timeline = reinterpret_cast<unsigned long long*>(d_timeline);
     ctx->c.timeline_rows = d_timeline ? rows : 0;
     return GMAPF_OK;
@@ -890,9 +898,10 @@ gmapf_status gmapf_search_batch_device(gmapf_ctx* ctx, const int32_t* d_starts, 
     if (n < 0 || path_stride < 1) return fail(GMAPF_E_INVALID_ARG, "bad sizes");
     if (n > 0 && (!d_starts || !d_targets || !d_found || !d_lens || !d_paths))
         return fail(GMAPF_E_INVALID_ARG, "null device pointer");
-    if (n > 0 && !(gpu_reachable(d_starts) && gpu_reachable(d_targets) && gpu_reachable(d_found) &&
-                   gpu_reachable(d_lens) && gpu_reachable(d_paths)))
-        return fail(GMAPF_E_INVALID_ARG, "a buffer is not GPU memory (device, managed or mapped pinned)");
+    const int dv = c.opt.device;
+    if (n > 0 && !(gpu_reachable(d_starts, dv) && gpu_reachable(d_targets, dv) && gpu_reachable(d_found, dv) &&
+                   gpu_reachable(d_lens, dv) && gpu_reachable(d_paths, dv)))
+        return fail(GMAPF_E_INVALID_ARG, "a buffer is not memory the context's GPU can reach (its device memory, managed or mapped pinned)");
     gmapf_status s = start_if_needed(c);
     if (s != GMAPF_OK) return s;
     std::string err;
@@ -1092,6 +1101,7 @@ gmapf_status gmapf_batch_create(gmapf_ctx* const* scenes, int32_t n, const gmapf
         if (opt->visited_mode < 0 || opt->visited_mode > 3)
             return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
         if (opt->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
+        if (opt->round_limit < 0) return fail(GMAPF_E_INVALID_ARG, "round_limit must be >= 0");
     }
     gmapf_batch* b = new (std::nothrow) gmapf_batch();
     gmapf_ctx* w = new (std::nothrow) gmapf_ctx();

@@ -35,6 +35,20 @@ namespace gmapf_b200 {
         }                                                                            \
     } while (0)
 
+// "device-side check failed: ..." with the names of the error bits set
+std::string device_error_text(int e) {
+    std::string s = "device-side check failed:";
+    if (e & ERR_ROUNDS) s += " a search reached the round limit;";
+    if (e & ERR_PATH_CAP) s += " a path did not fit its output row;";
+    if (e & ERR_BAD_REQUEST) s += " a request named a triangle outside the map;";
+    if (e & ERR_BOUNDS) s += " an index failed its bounds check;";
+    return s + " (error bits " + std::to_string(e) + ")";
+}
+
+int search_round_limit(const Context& c) {
+    return c.opt.round_limit > 0 ? c.opt.round_limit : 4 * c.map.n + 64;
+}
+
 namespace {
 
 // device counters: [8] holds the frame's dt as a float
@@ -85,7 +99,7 @@ SearchParams search_params(Context& c) {
     p.slots = d.slots;
     p.gbm = d.gbm;
     p.work_ctr = d.counters + CT_WORK;
-    p.max_rounds = 4 * c.map.n + 64;
+    p.max_rounds = search_round_limit(c);
     p.paths = d.paths;
     p.path_stride = d.path_stride;
     p.ag_state = d.state;
@@ -677,6 +691,7 @@ int device_wait_step(Context& c, std::string& err) {
     st.claims = (int64_t)delta[ST_CLAIMS];
     st.path_nodes = (int64_t)delta[ST_PATH_NODES];
     st.moving = (int64_t)delta[ST_MOVING];
+    st.neighbours = (int64_t)delta[ST_NEIGHBOURS];
     st.ms_step_wall = std::chrono::duration<float, std::milli>(t2 - c.t_step0).count();
     st.ms_search = st.ms_mover = st.ms_total_device = 0;
     if (c.cfg.IsProfiler) {
@@ -719,7 +734,7 @@ int device_wait_step(Context& c, std::string& err) {
         return GMAPF_E_DEVICE;
     }
     if (e != 0) {
-        err = "device-side check failed (error bits " + std::to_string(e) + ")";
+        err = device_error_text(e);
         return GMAPF_E_DEVICE;
     }
     return GMAPF_OK;
@@ -865,7 +880,7 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
     for (int k = 0; k < ST_COUNT; k++) c.stats_prev[k] += c.h_stats[k] - before[k];
     const int e = c.h_small[CT_ERR];
     if (e != 0) {
-        err = "device-side check failed (error bits " + std::to_string(e) + ")";
+        err = device_error_text(e);
         return (e & ERR_BAD_REQUEST) ? GMAPF_E_INVALID_ARG : GMAPF_E_DEVICE;
     }
     return GMAPF_OK;

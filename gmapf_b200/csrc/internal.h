@@ -37,6 +37,7 @@ enum StatIdx {
     ST_FOUND,
     ST_REQUESTS,
     ST_MOVING,
+    ST_NEIGHBOURS,  // agents examined in the 3x3 grid cells by the collision pass
     ST_COUNT
 };
 
@@ -366,6 +367,11 @@ struct Context {
 };
 
 // device.cu
+// rounds one search may run: the round_limit option, else 4 N + 64 (never
+// reached: every round pops a queued node and a node is queued once)
+int search_round_limit(const Context& c);
+// "device-side check failed: ..." naming the ErrBits set in e
+std::string device_error_text(int e);
 int device_start(Context& c, std::string& err);
 void device_free(Context& c);
 int device_async_step(Context& c, float dt, std::string& err);
@@ -400,5 +406,9 @@ int serve_result(Context& c, int agent, int* found, int* len, int* path, int cap
 
 // capi.cpp: message returned by gmapf_last_error() on this thread
 void set_last_error(const std::string& msg);
+// capi.cpp: p is memory a kernel on `device` may access (that GPU's device
+// memory, managed memory or mapped host memory); false for pageable host
+// memory and for another GPU's device memory
+bool gpu_reachable(const void* p, int device);
 
 }  // namespace gmapf_b200

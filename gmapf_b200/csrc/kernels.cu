@@ -320,6 +320,7 @@ __global__ void k_collide_progress(MoverParams p) {
     const float2 me = p.pos_mid[i];
     float2 np = me;
     const int c = p.cell_of[i];
+    unsigned examined = 0;  // agents of the 3x3 cells read (the agent itself included)
     if (c >= 0) {
         const int lc = c - sc.cell_base;  // cell within the agent's scene
         const int cx = lc % sc.aw, cy = lc / sc.aw;
@@ -332,6 +333,7 @@ __global__ void k_collide_progress(MoverParams p) {
         for (int yy = y0; yy <= y1; yy++)
             for (int xx = x0; xx <= x1; xx++) {
                 const int cc = sc.cell_base + yy * sc.aw + xx;
+                examined += p.cell_start[cc + 1] - p.cell_start[cc];
                 for (int k = p.cell_start[cc], e = p.cell_start[cc + 1]; k < e; k++) {
                     const int j = p.cell_items[k];
                     if (j == i) continue;
@@ -408,6 +410,11 @@ __global__ void k_collide_progress(MoverParams p) {
         }
     }
     p.pos[i] = np;
+    {  // counter of the agents examined (the mover's per-agent traffic), one atomic per warp
+        const unsigned m = __activemask();
+        const unsigned tot = __reduce_add_sync(m, examined);
+        if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(p.stats + ST_NEIGHBOURS, (unsigned long long)tot);
+    }
 
     if (!p.in_move[i]) return;
     // path progress

@@ -12,25 +12,29 @@
 //
 // That array (g_scratch, kScratchBytes) is a file-scope __device__ array:
 // every GPU that loads the library holds it until the process exits.  It
-// holds the search records of the concurrent request slots (32 bytes per
-// navmesh triangle per slot) and a small header (work counter, epoch
-// counter).  Calls share it and it keeps the previous call's contents:
-// the work counter is cleared by each call, and records are stamped with a
-// counter that never repeats, so stale records are never mistaken for live
-// ones.  Two calls that overlap on the GPU (different streams, or different
-// host threads) race on it and give wrong results: serialize them.
+// holds a small header (work counter, query counter) and the search records
+// of the concurrent request slots (32 bytes per navmesh triangle per slot).
+// Calls share it and it keeps the previous call's contents: the work counter
+// is cleared by each call, and records are stamped with a 64-bit query
+// number that never repeats (it would take centuries of queries to wrap), so
+// a stale record is never mistaken for a live one, whatever the earlier
+// calls' navmesh sizes were.  Two calls that overlap on the GPU (different
+// streams, or different host threads) race on it and give wrong results:
+// serialize them.
 //
 // The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current) and sets the kernel's
-// shared-memory limit; make that first call before any stream capture.
+// (cudaGetSymbolAddress, with that device current), clears it and sets the
+// kernel's shared-memory limit for its (threads per agent, queue capacity);
+// make that first call, and the first call with each new shape, before any
+// stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "internal.h"
-#include "records.cuh"
 
 namespace gmapf_b200 {
 namespace {
@@ -39,8 +43,8 @@ constexpr size_t kScratchBytes = size_t(64) << 20;  // 64 MiB per device
 constexpr size_t kHeaderBytes = 256;
 constexpr int kMaxDevices = 64;
 
-// header words
-enum { HD_WORK = 0, HD_EPOCH = 1 };
+// header: 32-bit work counter at byte 0, 64-bit query counter at byte 8
+constexpr size_t kWorkOff = 0, kQueryOff = 8;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -48,13 +52,39 @@ struct DeviceSetup {
     bool ready = false;
     unsigned char* scratch = nullptr;  // device address of g_scratch
     int sms = 0;
-    long long issued = 0;               // queries stamped since the last record wipe
+    std::unordered_map<int, int> blocks_per_sm;  // (T, C) -> resident one-warp blocks per SM
 };
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mu;
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kEntry = 8;  // F, G<<1|dir, id, five ancestors
+// queue / frontier entry: F, G<<1|dir, id, ancestors 1..4
+constexpr int kEntry = 7;
+
+// Search record of this kernel: the 64-bit stamp of the query that claimed
+// the node, G<<1|dir and ancestors 1..5 (anc[0] is the parent).  32 bytes,
+// read and written as one sector like the library's other records.
+struct __align__(32) NRec {
+    unsigned lo, hi;
+    int gd;
+    int anc[5];
+};
+static_assert(sizeof(NRec) == 32, "one sector per record");
+
+__device__ __forceinline__ int4 ld_head(const NRec* r) {  // {stamp lo, stamp hi, gd, parent}
+    return __ldcg(reinterpret_cast<const int4*>(r));
+}
+__device__ __forceinline__ void ld_nrec(const NRec* r, int4& a, int4& b) {
+    asm volatile("ld.global.cg.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                 : "l"(r));
+}
+__device__ __forceinline__ void st_nrec(NRec* r, unsigned long long stamp, int gd, int a0, int a1, int a2, int a3,
+                                        int a4) {
+    asm volatile("st.global.cg.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"((unsigned)stamp),
+                 "r"((unsigned)(stamp >> 32)), "r"(gd), "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(a4)
+                 : "memory");
+}
 
 __device__ __forceinline__ bool less3(float fa, int ga, int ia, float fb, int gb, int ib) {
     if (fa != fb) return fa < fb;
@@ -78,6 +108,7 @@ struct NoAllocArgs {
     int nq;
     int T, C;
     float K;
+    int max_rounds;
     int* found;
     int* lens;
     int* paths;
@@ -87,7 +118,8 @@ struct NoAllocArgs {
 };
 
 // One warp per request; the same rounds, claim order and queue rules as the
-// main search kernel, with the visited state in stamped scratch records.
+// main search kernel (include/gmapf/PathFinder.h:138-251 with the (F, G, id)
+// order), with the visited state in stamped scratch records.
 template <int T>
 __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
     constexpr int NP = (3 * T + 31) / 32;
@@ -99,8 +131,9 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
     const int qwords = kEntry * C * T;
     int* q = sm + wib * (qwords + kEntry * 3 * T);  // ring: word w of entry k of lane l at [(w*C+k)*T+l]
     int* fr = q + qwords;                           // frontier: word w of item i at [w*3T+i]
-    unsigned* hdr = reinterpret_cast<unsigned*>(a.scratch);
-    Rec* rec = reinterpret_cast<Rec*>(a.scratch + kHeaderBytes) + (size_t)slot * n_nodes;
+    unsigned* work = reinterpret_cast<unsigned*>(a.scratch + kWorkOff);
+    unsigned long long* qctr = reinterpret_cast<unsigned long long*>(a.scratch + kQueryOff);
+    NRec* rec = reinterpret_cast<NRec*>(a.scratch + kHeaderBytes) + (size_t)slot * n_nodes;
     const unsigned lt = (1u << lane) - 1u;
 
     auto at = [&](int k) { return (k >= C ? k - C : k) * T + (lane < T ? lane : 0); };
@@ -112,7 +145,7 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
 
     for (;;) {
         int r = 0;
-        if (lane == 0) r = atomicAdd(hdr + HD_WORK, 1);
+        if (lane == 0) r = atomicAdd(work, 1);
         r = __shfl_sync(kFull, r, 0);
         if (r >= a.nq) break;
         const int start = a.starts[r], target = a.targets[r];
@@ -123,24 +156,26 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
             }
             continue;
         }
-        unsigned ep = 0;
-        if (lane == 0) ep = atomicAdd(hdr + HD_EPOCH, 1u) + 1u;  // never repeats between wipes
+        unsigned long long ep = 0;
+        if (lane == 0) ep = atomicAdd(qctr, 1ull) + 1ull;  // never repeats: stale records never match
         ep = __shfl_sync(kFull, ep, 0);
+        const unsigned ep_lo = (unsigned)ep, ep_hi = (unsigned)(ep >> 32);
         const float2 cs = node_centroid(a.nodes, start), ct = node_centroid(a.nodes, target);
         const float f0 = __fmul_rn(dist_sqr(cs.x, cs.y, ct.x, ct.y), a.K);
         int beg = 0, size = 0;
-        if (lane < 2) {
+        if (lane < 2) {  // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
             const int node = lane == 0 ? start : target;
             const int k = at(0);
             q[k] = __float_as_int(f0);
             q[C * T + k] = lane == 0 ? 1 : 0;
             q[2 * C * T + k] = node;
-            for (int j = 0; j < 5; j++) q[(3 + j) * C * T + k] = -1;
+            for (int j = 0; j < 4; j++) q[(3 + j) * C * T + k] = -1;
             size = 1;
-            st_rec(rec + node, ep, lane == 0 ? 1 : 0, -1, -1, -1, -1, -1, -1);
+            st_nrec(rec + node, ep, lane == 0 ? 1 : 0, -1, -1, -1, -1, -1);
         }
         __syncwarp();
         int found = 0, mS = 0, gS = 0, mT = 0, gT = 0, rounds = 0;
+        bool capped = false;
         for (;;) {
             rounds++;
             int idu = -1, gdu = 0, uk = 0;
@@ -172,9 +207,9 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
                 bool prev = false;
                 int pgd = 0;
                 if (valid) {
-                    const int2 st = __ldcg(reinterpret_cast<const int2*>(rec + n));
-                    prev = (unsigned)st.x == ep;
-                    pgd = st.y;
+                    const int4 h = ld_head(rec + n);
+                    prev = (unsigned)h.x == ep_lo && (unsigned)h.y == ep_hi;
+                    pgd = h.z;
                 }
                 const bool fresh = valid && !prev;
                 const unsigned mm = __match_any_sync(kFull, fresh ? n : (-1 - lane));
@@ -205,14 +240,14 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
                     const float2 cn = node_centroid(a.nodes, n);
                     const float2 far = du ? ct : cs;
                     const float F = __fadd_rn((float)(ngd >> 1), __fmul_rn(dist_sqr(cn.x, cn.y, far.x, far.y), a.K));
-                    int ua[5];
-                    for (int j = 0; j < 5; j++) ua[j] = q[(3 + j) * C * T + cuk];
+                    int ua[4];
+                    for (int j = 0; j < 4; j++) ua[j] = q[(3 + j) * C * T + cuk];
                     fr[idx] = __float_as_int(F);
                     fr[3 * T + idx] = ngd;
                     fr[6 * T + idx] = n;
                     fr[9 * T + idx] = cu;
-                    for (int j = 0; j < 4; j++) fr[(4 + j) * 3 * T + idx] = ua[j];
-                    st_rec(rec + n, ep, ngd, cu, ua[0], ua[1], ua[2], ua[3], ua[4]);
+                    for (int j = 0; j < 3; j++) fr[(4 + j) * 3 * T + idx] = ua[j];
+                    st_nrec(rec + n, ep, ngd, cu, ua[0], ua[1], ua[2], ua[3]);
                 }
                 nwin += __popc(wm);
                 __syncwarp();
@@ -262,7 +297,10 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
                     }
                 }
                 if (!__any_sync(kFull, size > 0)) ended = true;
-                if (rounds >= 4 * n_nodes + 64) ended = true;
+                if (!ended && rounds >= a.max_rounds) {  // the round limit: reported as found = -2
+                    ended = true;
+                    capped = true;
+                }
             }
             __syncwarp();
             if (ended) break;
@@ -271,6 +309,9 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
         if (found) {
             L = gS + gT + 1;
             if ((long long)L <= a.stride && lane < 2) {
+                // lane 0: start side, depths gS..1 at positions gS-1..0;
+                // lane 1: target side, depths gT..0 at positions gS..gS+gT;
+                // each record read gives five more ancestors
                 int* out = a.paths + (long long)r * a.stride;
                 int x = lane == 0 ? mS : mT, g = lane == 0 ? gS : gT;
                 const int stop = lane == 0 ? 1 : 0;
@@ -281,23 +322,23 @@ __global__ void __launch_bounds__(32) k_search_noalloc(NoAllocArgs a) {
                 }
                 while (g > stop && x >= 0 && x < n_nodes) {
                     int4 p0, p1;
-                    ld_rec(rec + x, p0, p1);
-                    const int anc[6] = {p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-                    for (int j = 0; j < 6; j++) {
+                    ld_nrec(rec + x, p0, p1);
+                    const int anc[5] = {p0.w, p1.x, p1.y, p1.z, p1.w};
+                    for (int j = 0; j < 5; j++) {
                         const int d = g - 1 - j;
                         if (d >= stop) {
                             if (lane == 0) out[d - 1] = anc[j];
                             else out[gS + gT - d] = anc[j];
                         }
                     }
-                    x = anc[5];
-                    g -= 6;
+                    x = anc[4];
+                    g -= 5;
                 }
             }
         }
         __syncwarp();
         if (lane == 0) {
-            a.found[r] = found;
+            a.found[r] = capped ? -2 : found;
             a.lens[r] = L;  // a length above path_stride means the row was left unwritten
         }
     }
@@ -352,16 +393,16 @@ using namespace gmapf_b200;
 extern "C" gmapf_status gmapf_search_batch_noalloc(const gmapf_node* d_nodes, int32_t n_nodes,
                                                    const int32_t* d_starts, const int32_t* d_targets,
                                                    int32_t n_queries, int32_t threads_per_agent,
-                                                   int32_t queue_capacity, float heuristic_k, int32_t* d_found,
-                                                   int32_t* d_lens, int32_t* d_paths, int32_t path_stride,
-                                                   void* stream) {
+                                                   int32_t queue_capacity, float heuristic_k,
+                                                   int32_t round_limit, int32_t* d_found, int32_t* d_lens,
+                                                   int32_t* d_paths, int32_t path_stride, void* stream) {
     const int T = threads_per_agent, C = queue_capacity;
     if (!(T == 2 || T == 4 || T == 8 || T == 16 || T == 32))
         return fail(GMAPF_E_INVALID_ARG, "threads_per_agent must be one of 2, 4, 8, 16, 32");
     if (C < 1 || C > 512) return fail(GMAPF_E_INVALID_ARG, "queue_capacity must be in [1, 512]");
-    if (n_nodes < 1 || n_queries < 0 || path_stride < 1)
-        return fail(GMAPF_E_INVALID_ARG, "need n_nodes >= 1, n_queries >= 0, path_stride >= 1");
-    if ((size_t)n_nodes * sizeof(Rec) > kScratchBytes - kHeaderBytes)
+    if (n_nodes < 1 || n_queries < 0 || path_stride < 1 || round_limit < 0)
+        return fail(GMAPF_E_INVALID_ARG, "need n_nodes >= 1, n_queries >= 0, path_stride >= 1, round_limit >= 0");
+    if ((size_t)n_nodes * sizeof(NRec) > kScratchBytes - kHeaderBytes)
         return fail(GMAPF_E_CAPACITY,
                     "navmesh too large for the built-in 64 MiB scratch (at most 2,097,144 triangles)");
     if (n_queries > 0 && (!d_nodes || !d_starts || !d_targets || !d_found || !d_lens || !d_paths))
@@ -374,7 +415,16 @@ extern "C" gmapf_status gmapf_search_batch_noalloc(const gmapf_node* d_nodes, in
         cudaGetLastError();
         return fail(GMAPF_E_CUDA, "no usable current CUDA device");
     }
+    // a kernel given pageable host memory or another GPU's memory would
+    // fault: refuse it here (the check allocates nothing)
+    const void* bufs[6] = {d_nodes, d_starts, d_targets, d_found, d_lens, d_paths};
+    for (const void* b : bufs)
+        if (!gpu_reachable(b, dev))
+            return fail(GMAPF_E_INVALID_ARG,
+                        "a buffer is not memory the current GPU can reach (its device memory, managed or mapped "
+                        "pinned)");
     DeviceSetup* ds = &g_setup[dev];
+    int per_sm = 0;
     {
         std::lock_guard<std::mutex> lk(g_setup_mu);
         if (!ds->ready) {  // once per device, with that device current
@@ -388,36 +438,31 @@ extern "C" gmapf_status gmapf_search_batch_noalloc(const gmapf_node* d_nodes, in
                 cudaGetLastError();
                 return fail(GMAPF_E_CUDA, "cudaDeviceGetAttribute failed");
             }
-            ds->scratch = static_cast<unsigned char*>(ptr);
-            ds->issued = 0;
-            // records start unclaimed: zero them once (epochs start at 1)
-            if (cudaMemsetAsync(ds->scratch, 0, kScratchBytes, s) != cudaSuccess) {
+            // records start unclaimed: zero them once (query stamps start at 1)
+            if (cudaMemsetAsync(ptr, 0, kScratchBytes, s) != cudaSuccess) {
                 cudaGetLastError();
                 return fail(GMAPF_E_CUDA, "clearing the scratch array failed");
             }
+            ds->scratch = static_cast<unsigned char*>(ptr);
             ds->ready = true;
         }
+        // the kernel attribute and occupancy query run once per (T, C) on
+        // this device; later calls make no CUDA calls besides the launch
+        const int key = T * 1024 + C;
+        auto it = ds->blocks_per_sm.find(key);
+        if (it == ds->blocks_per_sm.end()) it = ds->blocks_per_sm.emplace(key, occupancy_any(T, C)).first;
+        per_sm = it->second;
     }
-    const int per_sm = occupancy_any(T, C);  // also raises the kernel's shared-memory limit
     if (per_sm <= 0) return fail(GMAPF_E_CAPACITY, "queues do not fit in shared memory for this T and C");
-    const long long by_mem = (long long)((kScratchBytes - kHeaderBytes) / ((size_t)n_nodes * sizeof(Rec)));
+    const long long by_mem = (long long)((kScratchBytes - kHeaderBytes) / ((size_t)n_nodes * sizeof(NRec)));
     long long slots = (long long)ds->sms * per_sm;  // one warp (one request slot) per block
     slots = std::min(slots, by_mem);
     slots = std::min(slots, (long long)n_queries);
     if (slots < 1) slots = 1;
     const int blocks = (int)slots;
 
-    // epoch stamps are 32-bit: wipe the records long before they could repeat
-    if (ds->issued + n_queries > (1ll << 31)) {
-        if (cudaMemsetAsync(ds->scratch, 0, kScratchBytes, s) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(GMAPF_E_CUDA, "clearing the scratch array failed");
-        }
-        ds->issued = 0;
-    }
-    ds->issued += n_queries;
     // the work counter must start at zero for every call
-    if (cudaMemsetAsync(ds->scratch + HD_WORK * sizeof(unsigned), 0, sizeof(unsigned), s) != cudaSuccess) {
+    if (cudaMemsetAsync(ds->scratch + kWorkOff, 0, sizeof(unsigned), s) != cudaSuccess) {
         cudaGetLastError();
         return fail(GMAPF_E_CUDA, "clearing the work counter failed");
     }
@@ -430,6 +475,9 @@ extern "C" gmapf_status gmapf_search_batch_noalloc(const gmapf_node* d_nodes, in
     a.T = T;
     a.C = C;
     a.K = heuristic_k;
+    // the default limit, 4 n + 64 rounds, is never reached: every round pops
+    // a queued node, and a node is queued at most once (when it is claimed)
+    a.max_rounds = round_limit > 0 ? round_limit : (int)std::min<long long>(4ll * n_nodes + 64, 0x7fffffff);
     a.found = d_found;
     a.lens = d_lens;
     a.paths = d_paths;

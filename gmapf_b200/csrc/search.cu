@@ -517,8 +517,9 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 pop_tail = have && best < 0;  // otherwise the ring is untouched by the pop
 #pragma unroll
                 for (int j = 0; j < 3; j++) pv[j] = pv[j] && j != best;  // the rest waits for insertion
-                if (!__any_sync(kFull, uid >= 0)) ended = true;
-                if ((int)rounds >= p.max_rounds) {
+                if (!__any_sync(kFull, uid >= 0))
+                    ended = true;
+                else if ((int)rounds >= p.max_rounds) {  // still running after its last allowed round
                     if (lane == 0) atomicOr(p.err, ERR_ROUNDS);
                     ended = true;
                 }

@@ -246,7 +246,7 @@ SearchParams serve_params(Context& c, Service& sv, int k) {
     p.gbm = sv.gbm;
     p.slot_base = k * sv.slots_per_stream;
     p.slots = sv.slots_per_stream;
-    p.max_rounds = 4 * c.map.n + 64;
+    p.max_rounds = search_round_limit(c);
     p.paths = sv.d_pool;
     p.path_stride = sv.stride;
     p.out_found = sv.d_found;
@@ -357,7 +357,7 @@ int admit_and_launch(Context& c, Service& sv, std::string& err) {
         if (!sv.st_busy[k] || cudaEventQuery(sv.st_done[k]) != cudaSuccess) continue;
         sv.st_busy[k] = false;
         if (sv.h_err[k] != 0) {
-            err = "serving search: device-side check failed (error bits " + std::to_string(sv.h_err[k]) + ")";
+            err = "serving search: " + device_error_text(sv.h_err[k]);
             sv.h_err[k] = 0;
             return GMAPF_E_DEVICE;
         }

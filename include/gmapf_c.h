@@ -28,7 +28,7 @@ typedef enum gmapf_status {
     GMAPF_E_INVALID_POS = 2,    /* a position lies in no navmesh triangle */
     GMAPF_E_CUDA = 3,           /* a CUDA runtime call failed */
     GMAPF_E_CAPACITY = 4,       /* a fixed capacity would be exceeded */
-    GMAPF_E_DEVICE_TIMEOUT = 5, /* a device-side wait ran out of iterations */
+    GMAPF_E_DEVICE_TIMEOUT = 5, /* a wait for device work ran out of time (gmapf_serve_drain) */
     GMAPF_E_INVALID_ARG = 6,    /* bad argument (null pointer, out-of-range id or parameter) */
     GMAPF_E_UNSUPPORTED = 7,    /* feature not compiled in (e.g. the CDT navmesh builder) */
     GMAPF_E_DEVICE = 8          /* a device-side check failed (bounds / consistency) */
@@ -94,7 +94,12 @@ typedef struct gmapf_options {
                                   instead of triangle centroids; the triangle paths and the per-triangle
                                   progress stay the reference's.  Off (0) by default: on, agents take
                                   different routes from the reference's (AgentsMover.h:148,174) */
-    int32_t _reserved[3];
+    int32_t round_limit;       /* rounds one search may run before it is stopped, not found, and the
+                                  call or step reports GMAPF_E_DEVICE (round-limit bit); 0 = 4 N + 64
+                                  for an N-triangle map, which no search reaches (every round pops a
+                                  queued node and a node is queued once).  Smaller values bound the
+                                  time of one search */
+    int32_t _reserved[2];
 } gmapf_options;
 
 typedef struct gmapf_step_stats {
@@ -110,6 +115,7 @@ typedef struct gmapf_step_stats {
     float ms_search;        /* device time of the search kernel(s) */
     float ms_mover;         /* device time of the mover kernels */
     float ms_total_device;  /* device time of the whole frame */
+    int64_t neighbours;     /* agents read from the 3x3 grid cells by the collision pass (summed over agents) */
 } gmapf_step_stats;
 
 typedef struct gmapf_ctx gmapf_ctx;
@@ -356,22 +362,28 @@ int64_t gmapf_clock_ns(void);
  * of the call): no context, no cudaMalloc, no cudaFree.  The caller passes
  * the navmesh (n_nodes gmapf_node records, neighbours packed and -1 padded,
  * as for FillMapManually; centroids are recomputed), the start/target
- * triangle ids and the outputs, all in device memory; results equal
+ * triangle ids and the outputs, all in memory the current GPU can reach
+ * (its device memory, managed or mapped pinned; anything else is refused with
+ * GMAPF_E_INVALID_ARG before a launch); results equal
  * gmapf_search_batch_device's for the same threads per agent and queue
- * capacity.  found[i] is 1, 0, or -1 for an id outside the navmesh; a length
- * above path_stride means path row i was left unwritten.
+ * capacity.  found[i] is 1 (found), 0 (not found), -1 for an id outside the
+ * navmesh, or -2 when the search reached round_limit rounds before ending
+ * (round_limit 0 means the default, 4 n_nodes + 64, which no search
+ * reaches); a length above path_stride means path row i was left unwritten.
  * Working memory is one 64 MiB array built into the library (held by every
  * GPU that loads it until exit): the navmesh may have at most 2,097,144
  * triangles, and fewer triangles give more concurrent requests.  Calls share
  * that array: calls that overlap on the GPU race and must be serialized.
  * Enqueued on `stream` (a cudaStream_t, null for the default stream) and
- * asynchronous.  The first call on each device sets up the array's address
- * and the kernel attributes, so make it before any stream capture.  Errors
- * are read with gmapf_last_error(). */
+ * asynchronous.  The first call on each device sets up the array's address,
+ * and the first call with each (threads per agent, queue capacity) sets the
+ * kernel's shared-memory limit, so make those before any stream capture.
+ * Errors are read with gmapf_last_error(). */
 gmapf_status gmapf_search_batch_noalloc(const gmapf_node* d_nodes, int32_t n_nodes, const int32_t* d_starts,
                                         const int32_t* d_targets, int32_t n_queries, int32_t threads_per_agent,
-                                        int32_t queue_capacity, float heuristic_k, int32_t* d_found,
-                                        int32_t* d_lens, int32_t* d_paths, int32_t path_stride, void* stream);
+                                        int32_t queue_capacity, float heuristic_k, int32_t round_limit,
+                                        int32_t* d_found, int32_t* d_lens, int32_t* d_paths, int32_t path_stride,
+                                        void* stream);
 
 #ifdef __cplusplus
 }

@@ -541,6 +541,9 @@ void orc_map_centroids(const orc_map* m, float* out) {
 
 int orc_locate_linear(const orc_map* m, float x, float y) { return locate_linear(*m, x, y); }
 int orc_locate(const orc_map* m, float x, float y) { return locate(*m, x, y); }
+void orc_locate_batch(const orc_map* m, const float* xy, int n, int* out) {
+    for (int i = 0; i < n; i++) out[i] = locate(*m, xy[2 * i], xy[2 * i + 1]);
+}
 int orc_in_node(const orc_map* m, float x, float y, int node) {
     return point_in_tri(&m->t[6 * node], x, y) ? 1 : 0;
 }

@@ -54,6 +54,16 @@ int orc_map_count(const orc_map* m);
 void orc_map_centroids(const orc_map* m, float* out_xy);
 int orc_locate_linear(const orc_map* m, float x, float y);
 int orc_locate(const orc_map* m, float x, float y);
+/* orc_locate for n points (xy interleaved) */
+void orc_locate_batch(const orc_map* m, const float* xy, int n, int* out);
+
+/* Navmesh of a FillMapStart(size) + FillMapObstacle(...) + FillMapEnd()
+ * sequence (navmesh_oracle.cpp): obstacle o has obst_counts[o] vertices,
+ * taken in order from obst_xy (xy interleaved).  Writes 6 floats and 3
+ * neighbour ids per triangle and returns the triangle count; -1 when it
+ * exceeds cap, -2 when built without the CDT headers, -3 when CDT fails. */
+int orc_navmesh_build(float size_x, float size_y, const float* obst_xy, const int* obst_counts, int n_obst,
+                      float* out_tri, int* out_nbr, int cap);
 int orc_in_node(const orc_map* m, float x, float y, int node);
 float orc_dist_sqr(const orc_map* m, int a, int b);
 

@@ -8,6 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -37,10 +38,13 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    src = [HERE / "gmapf_oracle.cpp", HERE / "gmapf_oracle.h"]
+    src = [HERE / "gmapf_oracle.cpp", HERE / "gmapf_oracle.h", HERE / "navmesh_oracle.cpp", HERE / "Makefile"]
     if (not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in src)) and \
             os.environ.get("GMAPF_NO_BUILD") != "1":
-        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+        sys.path.insert(0, str(HERE.parent))
+        from gmapf_b200 import build as _build  # the build recipe only (where the CDT headers are)
+        cdt = _build.cdt_dir()
+        subprocess.run(["make", "-s", "-C", str(HERE)] + ([f"CDT_DIR={cdt}"] if cdt else []), check=True)
     lib = C.CDLL(str(LIB))
     sig = {
         "orc_map_create": (C.c_void_p, [F, I, C.c_int]),
@@ -49,6 +53,8 @@ def load():
         "orc_map_centroids": (None, [C.c_void_p, F]),
         "orc_locate_linear": (C.c_int, [C.c_void_p, C.c_float, C.c_float]),
         "orc_locate": (C.c_int, [C.c_void_p, C.c_float, C.c_float]),
+        "orc_locate_batch": (None, [C.c_void_p, F, C.c_int, I]),
+        "orc_navmesh_build": (C.c_int, [C.c_float, C.c_float, F, I, C.c_int, F, I, C.c_int]),
         "orc_in_node": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_int]),
         "orc_dist_sqr": (C.c_float, [C.c_void_p, C.c_int, C.c_int]),
         "orc_search": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, I, C.c_int, I,
@@ -79,6 +85,25 @@ def load():
         f.argtypes = a
     _lib = lib
     return lib
+
+
+def navmesh(size, obstacles):
+    """(tri, nbr) of the navmesh FillMapStart(size), FillMapObstacle(o) for
+    each obstacle and FillMapEnd() build (the reference's CDT call sequence,
+    oracle/navmesh_oracle.cpp)."""
+    lib = load()
+    xy = np.ascontiguousarray(np.concatenate([np.asarray(o, np.float32).reshape(-1, 2) for o in obstacles])
+                              if obstacles else np.zeros((0, 2), np.float32), np.float32)
+    counts = np.ascontiguousarray([len(o) for o in obstacles], np.int32)
+    cap = 4 * (len(xy) + 4) + 64
+    tri = np.empty((cap, 6), np.float32)
+    nbr = np.empty((cap, 3), np.int32)
+    n = lib.orc_navmesh_build(float(size[0]), float(size[1]), _p(xy, C.c_float), _p(counts), len(counts),
+                              _p(tri, C.c_float), _p(nbr), cap)
+    if n < 0:
+        raise RuntimeError({-1: "navmesh larger than expected", -2: "oracle built without the CDT headers",
+                            -3: "CDT failed"}.get(n, str(n)))
+    return tri[:n].copy(), nbr[:n].copy()
 
 
 def nodes_to_arrays(nodes):
@@ -114,6 +139,24 @@ class OMap:
     def locate(self, x, y, linear=False):
         f = self.lib.orc_locate_linear if linear else self.lib.orc_locate
         return f(self.h, float(x), float(y))
+
+    def locate_batch(self, pts):
+        """orc_locate for an (n, 2) array of points."""
+        p = np.ascontiguousarray(pts, np.float32).reshape(-1, 2)
+        out = np.empty(len(p), np.int32)
+        self.lib.orc_locate_batch(self.h, _p(p, C.c_float), len(p), _p(out))
+        return out
+
+    def free_points(self, size, n, rng):
+        """n points uniform over [0, W) x [0, H), kept when inside a triangle
+        (the rule of gmapf_b200.scenarios.free_points, located here)."""
+        W, H = size
+        out = np.empty((0, 2), np.float32)
+        while len(out) < n:
+            k = max(64, 2 * (n - len(out)))
+            p = np.stack([rng.uniform(0, W, k), rng.uniform(0, H, k)], 1).astype(np.float32)
+            out = np.concatenate([out, p[self.locate_batch(p) >= 0]])
+        return out[:n]
 
     def search(self, s, t, T, Cap, K=1.0):
         path = np.empty(max(1, self.n), np.int32)
