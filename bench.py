@@ -388,6 +388,29 @@ def serving(rates, duration_s: float, n_scenes: int = 8, agents: int = 8192):
     return out
 
 
+# ------------------------------------------------------- shared definitions --
+
+# Search shape (threads per agent, queue capacity) of the headline frames:
+# the shape the autotuner picks for these maps on B200 (T=32, C=16 on both
+# mazes).  Both arms run it: the GPU arm autotunes at the start and reports
+# its pick; should the pick differ, its headline still runs this shape (the
+# line says so), so the two arms always time the same method.
+TUNED_SHAPE = {160: (32, 16), 64: (32, 16)}
+
+
+def headline_shape(args):
+    if args.shape:
+        T, C = (int(x) for x in args.shape.split(","))
+        return T, C
+    return TUNED_SHAPE.get(args.cells, (args.threads_per_agent, args.queue_capacity))
+
+
+def workload_config(args, triangles, A, T, C):
+    """The `config` both arms print for the headline workload."""
+    return {"workload": f"maze {args.cells}x{args.cells} cells on 4000x4000, {A} agents, all retargeted every "
+                        f"frame", "triangles": triangles, "agents": A, "threads_per_agent": T, "queue_capacity": C}
+
+
 # --------------------------------------------------------------- b200 arm --
 
 def make_scene(cells, seed, T, C, mode, agents, profiler=True, autotune=False):
@@ -441,20 +464,41 @@ def run_frames_device(g, sets, warmup, steps, torch, flush):
 
 
 def run_frames_host(g, sets, warmup, steps):
-    """e2e: host buffers through the reference-facing API."""
+    """e2e: host buffers through the reference-facing API.  Per frame the host
+    wall time of each call (bulk SetAgentTargPos, AsyncStep, WaitStepEnd) and
+    the frame's device time (CUDA events inside the frame) are kept, so the
+    end-to-end tail can be attributed."""
     A = sets[0].shape[0]
     ids = np.arange(A, dtype=np.int32)
     wall, stats = [], []
+    parts = {"retarget": [], "async_step": [], "wait_step_end": [], "device": []}
     for k in range(warmup + steps):
         t0 = time.perf_counter()
         g.set_targets(ids, sets[k])
-        g.AsyncStep(1.0 / 60.0)
-        g.WaitStepEnd()
         t1 = time.perf_counter()
+        g.AsyncStep(1.0 / 60.0)
+        t2 = time.perf_counter()
+        g.WaitStepEnd()
+        t3 = time.perf_counter()
         if k >= warmup:
-            wall.append((t1 - t0) * 1e3)
-            stats.append(g.last_stats())
-    return wall, stats
+            wall.append((t3 - t0) * 1e3)
+            st = g.last_stats()
+            stats.append(st)
+            parts["retarget"].append((t1 - t0) * 1e3)
+            parts["async_step"].append((t2 - t1) * 1e3)
+            parts["wait_step_end"].append((t3 - t2) * 1e3)
+            parts["device"].append(st["ms_total_device"])
+    return wall, stats, parts
+
+
+def attribution(wall, parts):
+    """p50/p99 of each part of the host-API frame time (ms)."""
+    out = {"frames": len(wall), "total": {"p50": pct(wall, 50), "p99": pct(wall, 99)}}
+    for k, v in parts.items():
+        out[k] = {"p50": pct(v, 50), "p99": pct(v, 99), "mean": statistics.mean(v) if v else None}
+    out["host_over_device"] = {"p50": pct(wall, 50) - pct(parts["device"], 50),
+                               "p99": pct(wall, 99) - pct(parts["device"], 99)}
+    return out
 
 
 def path_quality(g, sample):
@@ -490,6 +534,113 @@ def cpu_baseline(g, scn, sets, T, C, sample, threads):
                       f"oracle/ C++ restatement, {threads} host threads"}
 
 
+def longest_query(g, starts, targets, torch):
+    """The frame's slowest search: found with the search timeline on a
+    frame-sized batch of the frame's queries (each request's start and end on
+    the GPU global timer), then timed alone (one-query batch, CUDA events,
+    best of 3).  Its time alone bounds any schedule of the frame from below."""
+    import gmapf_b200 as G
+    n = len(starts)
+    tl = torch.zeros(2 * n, dtype=torch.int64, device="cuda")
+    g.set_search_timeline(tl.data_ptr(), n)
+    try:
+        g.search_batch(starts, targets, 2)  # 2-entry rows: long paths raise the path-capacity flag
+    except G.GMAPFError:
+        pass
+    batch_ms = g.last_search_ms()
+    g.set_search_timeline(0, 0)
+    x = tl.cpu().numpy().reshape(n, 2)
+    dur = (x[:, 1] - x[:, 0]) / 1e6
+    i = int(np.argmax(dur))
+    alone, rounds = [], 0
+    for _ in range(3):
+        try:
+            g.search_batch(starts[i:i + 1], targets[i:i + 1], 2)
+        except G.GMAPFError:
+            pass
+        alone.append(g.last_search_ms())
+    st = g.search_batch(starts[i:i + 1], targets[i:i + 1], g.node_count)[3]
+    return {"query": i, "rounds": int(st["rounds"]), "path_len": int(st["path_nodes"]),
+            "alone_ms": min(alone), "in_batch_ms": float(dur[i]), "batch_ms": batch_ms,
+            "us_per_round_alone": 1e3 * min(alone) / max(1, st["rounds"]),
+            "us_per_round_in_batch": 1e3 * float(dur[i]) / max(1, st["rounds"])}
+
+
+def mover_roofline(stats, A, peak, peak_kind):
+    """The mover phase (k_move_bin, k_cell_scan, k_scatter, k_collide_progress)
+    against HBM: per agent per frame 64 + 16 B plus 8 B per agent read from
+    the 3x3 grid cells (the `neighbours` counter), over the mover's CUDA-event
+    time of the frames in which agents moved."""
+    fr = [s for s in stats if s["moving"] > 0 and s["ms_mover"] > 0]
+    if not fr:
+        return None
+    byt = sum(80.0 * A + 8.0 * s["neighbours"] for s in fr)
+    ms = sum(s["ms_mover"] for s in fr)
+    achieved = byt / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernels": "k_move_bin + k_cell_scan + k_scatter + k_collide_progress",
+            "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+            "algorithmic_bytes_per_frame": byt / len(fr), "mover_ms_per_frame": ms / len(fr),
+            "neighbours_per_agent": sum(s["neighbours"] for s in fr) / (len(fr) * A), "frames": len(fr)}
+
+
+def mover_cfg2(steps, peak, peak_kind):
+    """The reference's headline-scale configuration as specified (its TestFull
+    driver, main.cpp:45-86): 1000x1000 map with 200 rectangles, 2,048 agents
+    of radius 2 and speed 1, every agent retargeted to a fresh free point
+    every 100 steps, T=8, C=32, `steps` frames of 1/60 s through the host API."""
+    from gmapf_b200 import scenarios as S
+    import gmapf_b200 as G
+    scn = S.cfg2()
+    A = scn.agents
+    g, starts, rng = S.make_world(scn, agents=A, profiler=True)
+    g.ManualStart()
+    ids = np.arange(A, dtype=np.int32)
+    wall, stats = [], []
+    for k in range(steps):
+        t0 = time.perf_counter()
+        if k % scn.retarget_every == 0:
+            g.set_targets(ids, S.free_points(g, scn, A, rng))
+        t1 = time.perf_counter()
+        g.AsyncStep(scn.dt)
+        g.WaitStepEnd()
+        wall.append((time.perf_counter() - t1) * 1e3)
+        stats.append(g.last_stats())
+    out = {"workload": "1000x1000, 200 rectangles (sides 10-60), 2048 agents r=2 speed 1, all retargeted every "
+                       f"100 steps, T=8, C=32, {steps} steps", "triangles": g.node_count, "agents": A,
+           "steps": steps, "p50_step_ms": pct(wall, 50), "p99_step_ms": pct(wall, 99),
+           "agent_steps_per_s": A * steps / (sum(wall) / 1e3),
+           "device_ms_per_step": statistics.mean(s["ms_total_device"] for s in stats),
+           "moving_per_step": statistics.mean(s["moving"] for s in stats),
+           "roofline": mover_roofline(stats, A, peak, peak_kind)}
+    g.close()
+    return out
+
+
+def mover_frames(g, frames, torch, flush, peak, peak_kind):
+    """Frames with no retargets after the full-retarget frames: every agent
+    walks its path (and collides).  Host wall per frame, the frame's and the
+    mover's CUDA-event device time; L2 flushed between frames."""
+    A = g.agent_count
+    wall, stats = [], []
+    for k in range(frames):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.AsyncStep(1.0 / 60.0)
+        g.WaitStepEnd()
+        wall.append((time.perf_counter() - t0) * 1e3)
+        stats.append(g.last_stats())
+    mv = [s["ms_mover"] for s in stats]
+    return {"frames": frames, "agents": A, "p50_step_ms": pct(wall, 50), "p99_step_ms": pct(wall, 99),
+            "device_ms_per_step": {"p50": pct([s["ms_total_device"] for s in stats], 50),
+                                   "p99": pct([s["ms_total_device"] for s in stats], 99)},
+            "mover_ms_per_step": {"p50": pct(mv, 50), "p99": pct(mv, 99)},
+            "moving_per_step": statistics.mean(s["moving"] for s in stats),
+            "agent_steps_per_s": A * frames / (sum(wall) / 1e3),
+            "agent_steps_per_s_device": A * frames / (sum(s["ms_total_device"] for s in stats) / 1e3),
+            "roofline": mover_roofline(stats, A, peak, peak_kind)}
+
+
 def bench_b200(args):
     import torch
     ws, rank, local = dist_env()
@@ -498,16 +649,25 @@ def bench_b200(args):
     import gmapf_b200 as G
 
     A = args.agents
-    T, C = args.threads_per_agent, args.queue_capacity
+    Tc, Cc = args.threads_per_agent, args.queue_capacity  # the Config's shape (the plain form's)
+    Th, Ch = headline_shape(args)  # the headline shape, shared with the reference arm
     seed = 3 + rank
     autotune = not args.no_autotune
-    scn, g, rng = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A, autotune=autotune)
-    n_nodes = g.node_count
+    scn, g, rng = make_scene(args.cells, seed, Tc, Cc, G.MODE_BATCHED, A, autotune=autotune)
     shape = g.search_shape()
-    Tb, Cb = shape["T"], shape["C"]  # the batched form's shape (autotuned per map)
+    pick = (shape["T"], shape["C"])
+    shape_source = "autotuned per map" if autotune else "fixed"
+    if pick != (Th, Ch):
+        g.close()
+        scn, g, rng = make_scene(args.cells, seed, Th, Ch, G.MODE_BATCHED, A)
+        shape = g.search_shape()
+        shape_source = (f"the headline shape shared with the reference arm (the autotuner picked T={pick[0]}, "
+                        f"C={pick[1]})" if autotune else "fixed")
+    n_nodes = g.node_count
     K, W = args.steps, args.warmup
     sets = target_sets(g, scn, rng, W + K, A)
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    peak, peak_kind = measured_peaks()
 
     barrier(dist)
     with ClockSampler(local) as clk:
@@ -518,10 +678,8 @@ def bench_b200(args):
     all_queries = reduce_sum(dist, queries)
     value = all_queries / (dev_total_ms / 1e3)
 
-    # The extras below (path quality, many-frame percentiles, the Config-shape
-    # and plain forms, the CPU baseline, the multi-scene, serving and 64x64
-    # workloads) belong to the one-GPU line: a multi-GPU line carries the
-    # scaled metric only, so the GPUs of a scaling run are not held for them.
+    # The extras below belong to the one-GPU line: a multi-GPU line carries
+    # the scaled metric only, so the GPUs of a scaling run are not held for them.
     extras = ws == 1
 
     # path quality of the last device-timed frame (sample; outside the timing)
@@ -529,18 +687,24 @@ def bench_b200(args):
     if extras and args.quality_sample > 0:
         quality = path_quality(g, args.quality_sample)
 
+    # the frame's slowest search, alone (its time bounds the frame from below)
+    longest = None
+    if extras and args.longest:
+        d = g.debug_agents()
+        longest = longest_query(g, d["cur_node"].astype(np.int32), g.locate(sets[-1]).astype(np.int32), torch)
+
     # p99 over many full-retarget frames through the host API (fresh targets each)
     p99_long = None
     if extras and args.p99_frames > 0:
-        wl, _ = run_frames_host(g, target_sets(g, scn, rng, 3 + args.p99_frames, A), 3, args.p99_frames)
+        wl, _, parts_l = run_frames_host(g, target_sets(g, scn, rng, 3 + args.p99_frames, A), 3, args.p99_frames)
         p99_long = {"frames": args.p99_frames, "p50_step_ms": pct(wl, 50), "p99_step_ms": pct(wl, 99),
-                    "max_step_ms": max(wl)}
+                    "max_step_ms": max(wl), "attribution": attribution(wl, parts_l)}
 
     # e2e through the host API (fresh targets, same scene)
     sets_e2e = target_sets(g, scn, rng, W + K, A)
     g.reset_profiler()
     barrier(dist)
-    wall, hstats = run_frames_host(g, sets_e2e, W, K)
+    wall, hstats, parts = run_frames_host(g, sets_e2e, W, K)
     barrier(dist)
     e2e_total = reduce_max(dist, float(sum(wall)))
     e2e_q = reduce_sum(dist, float(sum(s["requests"] for s in hstats)))
@@ -550,35 +714,57 @@ def bench_b200(args):
     search_ms = [s["ms_search"] for s in dstats]
     ab = [algorithmic_bytes(s, n_nodes) for s in dstats]
     achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
-    peak, peak_kind = measured_peaks()
-    traffic, traffic_src = measured_traffic(args.cells, Tb, Cb, shape["visited_mode"], queries / max(1, K))
-    ipr, ipr_src = measured_inst_per_round(args.cells, Tb, Cb, shape["visited_mode"])
+    traffic, traffic_src = measured_traffic(args.cells, shape["T"], shape["C"], shape["visited_mode"],
+                                            queries / max(1, K))
+    ipr, ipr_src = measured_inst_per_round(args.cells, shape["T"], shape["C"], shape["visited_mode"])
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+
+    # frames in which every agent walks its path (the mover at the maze scale)
+    moving = None
+    if extras and args.mover_frames > 0:
+        moving = mover_frames(g, args.mover_frames, torch, flush, peak, peak_kind)
+        moving["workload"] = (f"maze {args.cells}x{args.cells}, {A} agents walking the paths of the last "
+                              f"full-retarget frame, no retargets")
 
     # batched form at the Config's own shape (same arithmetic as the plain form)
     fixed = None
-    if extras and autotune and (Tb, Cb) != (T, C) and not args.no_plain:
-        scn_f, gf, rng_f = make_scene(args.cells, seed, T, C, G.MODE_BATCHED, A)
+    if extras and (Th, Ch) != (Tc, Cc) and not args.no_plain:
+        scn_f, gf, rng_f = make_scene(args.cells, seed, Tc, Cc, G.MODE_BATCHED, A)
         msf, stf, _ = run_frames_device(gf, sets, W, K, torch, flush)
-        fixed = {"threads_per_agent": T, "queue_capacity": C, "unit": "path queries/s",
+        wf, hf, _ = run_frames_host(gf, sets_e2e, W, K)
+        fixed = {"threads_per_agent": Tc, "queue_capacity": Cc, "unit": "path queries/s",
                  "value": sum(s["requests"] for s in stf) / (sum(msf) / 1e3),
+                 "e2e_value": sum(s["requests"] for s in hf) / (sum(wf) / 1e3),
                  "device_ms_per_step": {"mean": statistics.mean(msf), "p99": pct(msf, 99)},
                  "found_rate": sum(s["found"] for s in stf) / max(1, sum(s["requests"] for s in stf))}
         gf.close()
 
-    # plain per-agent form on the same frames
-    plain = None
+    # plain per-agent form on the same frames, at both shapes
+    plain = {}
     if extras and not args.no_plain:
-        scn_p, gp, rng_p = make_scene(args.cells, seed, T, C, G.MODE_PLAIN, A)
-        pk = max(2, min(K, 5))
-        wall_p, pst = run_frames_host(gp, sets[:1 + pk], 1, pk)
-        plain = {"value": sum(s["requests"] for s in pst) / (sum(wall_p) / 1e3), "unit": "path queries/s",
-                 "p99_step_ms": pct(wall_p, 99), "ms_per_step": statistics.mean(wall_p), "steps": pk}
-        gp.close()
+        for (T, C) in sorted({(Th, Ch), (Tc, Cc)}):
+            scn_p, gp, rng_p = make_scene(args.cells, seed, T, C, G.MODE_PLAIN, A)
+            pk = max(2, min(K, 5))
+            wall_p, pst, _ = run_frames_host(gp, sets_e2e[:1 + pk], 1, pk)
+            plain[f"T{T}_C{C}"] = {"threads_per_agent": T, "queue_capacity": C,
+                                   "value": sum(s["requests"] for s in pst) / (sum(wall_p) / 1e3),
+                                   "unit": "path queries/s", "p99_step_ms": pct(wall_p, 99),
+                                   "ms_per_step": statistics.mean(wall_p), "steps": pk}
+            gp.close()
+    batched_over_plain = None
+    if plain:
+        batched_over_plain = {f"T{Th}_C{Ch}": e2e_value / plain[f"T{Th}_C{Ch}"]["value"]}
+        if fixed:
+            batched_over_plain[f"T{Tc}_C{Cc}"] = fixed["e2e_value"] / plain[f"T{Tc}_C{Cc}"]["value"]
+        batched_over_plain["note"] = ("host-API path queries/s of the batched form over the plain form at the "
+                                      "same threads per agent and queue capacity (the same searches)")
 
     cpu = None
     if extras and not args.no_cpu:  # on rank 0 at N=1 only
-        cpu = cpu_baseline(g, scn, sets, Tb, Cb, args.cpu_sample, os.cpu_count() or 1)
+        cpu = cpu_baseline(g, scn, sets, shape["T"], shape["C"], args.cpu_sample, os.cpu_count() or 1)
+
+    # the reference's headline-scale configuration, as specified (mover at scale)
+    cfg2 = mover_cfg2(args.cfg2_steps, peak, peak_kind) if extras and args.cfg2_steps > 0 else None
 
     # the multi-scene configuration (scene batch against separate contexts)
     multi = None
@@ -593,22 +779,31 @@ def bench_b200(args):
     # secondary workload: the 64x64-cell maze of the configuration text
     secondary = None
     if extras and args.secondary_cells and args.secondary_cells != args.cells:
-        scn2, g2, rng2 = make_scene(args.secondary_cells, 3, T, C, G.MODE_BATCHED, A, autotune=autotune)
+        scn2, g2, rng2 = make_scene(args.secondary_cells, 3, Tc, Cc, G.MODE_BATCHED, A, autotune=autotune)
         sh2 = g2.search_shape()
         sets2 = target_sets(g2, scn2, rng2, W + K, A)
         ms2, st2, _ = run_frames_device(g2, sets2, W, K, torch, flush)
-        wall2, _ = run_frames_host(g2, target_sets(g2, scn2, rng2, W + K, A), W, K)
+        wall2, _, parts2 = run_frames_host(g2, target_sets(g2, scn2, rng2, W + args.p99_frames_secondary,
+                                                           A), W, args.p99_frames_secondary)
+        d2 = g2.debug_agents()
+        lq2 = longest_query(g2, d2["cur_node"].astype(np.int32), g2.locate(sets2[-1]).astype(np.int32),
+                            torch) if args.longest else None
         secondary = {"workload": f"maze {args.secondary_cells}x{args.secondary_cells} cells",
                      "triangles": g2.node_count, "threads_per_agent": sh2["T"],
                      "queue_capacity": sh2["C"], "block_threads": sh2["block_threads"],
                      "value": sum(s["requests"] for s in st2) / (sum(ms2) / 1e3),
-                     "e2e_value": A * K / (sum(wall2) / 1e3), "p99_step_ms": pct(wall2, 99),
-                     "p50_step_ms": pct(wall2, 50), "ms_per_step_device": statistics.mean(ms2)}
+                     "e2e_value": A * len(wall2) / (sum(wall2) / 1e3), "p99_step_ms": pct(wall2, 99),
+                     "p50_step_ms": pct(wall2, 50), "ms_per_step_device": statistics.mean(ms2),
+                     "device_ms_per_step": {"p50": pct(ms2, 50), "p99": pct(ms2, 99)},
+                     "attribution": attribution(wall2, parts2), "longest_query": lq2}
         g2.close()
 
     if rank == 0:
         st_sum = {k: sum(s[k] for s in dstats) for k in ["requests", "found", "expansions", "rounds", "claims"]}
         clocks = clk.summary()
+        cfg = workload_config(args, n_nodes, A, shape["T"], shape["C"])
+        cfg.update({"l2": "flushed between frames (256 MB write); per-frame search records exceed L2",
+                    "parallelism": f"{ws} independent scenes (one per GPU)"})
         line = {
             "metric": METRIC,
             "value": value,
@@ -622,26 +817,28 @@ def bench_b200(args):
             "vs_baseline": None,
             "dtype": "f32+i32",
             "data": "synthetic: seeded randomized-DFS maze, uniform free-space starts and targets",
-            "config": {"workload": f"maze {args.cells}x{args.cells} cells on 4000x4000, {A} agents, all "
-                                   f"retargeted every frame", "triangles": n_nodes, "agents": A,
-                       "threads_per_agent": Tb, "queue_capacity": Cb, "block_threads": shape["block_threads"],
-                       "shape_source": "autotuned per map" if autotune else "Config",
-                       "start_s": round(g.startup_s, 2),
-                       "config_threads_per_agent": T, "config_queue_capacity": C,
-                       "visited_mode": VISITED[shape["visited_mode"]],
-                       "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",
-                       "l2": "flushed between frames (256 MB write); per-frame search records exceed L2",
-                       "parallelism": f"{ws} independent scenes (one per GPU)"},
+            "config": cfg,
+            "setup": {"block_threads": shape["block_threads"], "shape_source": shape_source,
+                      "autotuner_pick": {"threads_per_agent": pick[0], "queue_capacity": pick[1]},
+                      "start_s": round(g.startup_s, 2), "config_threads_per_agent": Tc,
+                      "config_queue_capacity": Cc, "visited_mode": VISITED[shape["visited_mode"]],
+                      "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)"},
             "p99_step_ms": pct(wall, 99),
             "p50_step_ms": pct(wall, 50),
-            "device_ms_per_step": {"mean": statistics.mean(ms), "p99": pct(ms, 99), "max": max(ms)},
+            "device_ms_per_step": {"mean": statistics.mean(ms), "p50": pct(ms, 50), "p99": pct(ms, 99),
+                                   "max": max(ms)},
             "found_rate": st_sum["found"] / max(1, st_sum["requests"]),
             "expansions_per_s": st_sum["expansions"] / (sum(ms) / 1e3),
-            "plain": plain,
+            "longest_query": longest,
+            "plain": plain or None,
             "batched_config_shape": fixed,
+            "batched_over_plain": batched_over_plain,
             "path_quality": quality,
+            "reference_cuda_build": "not run: its claim race can feed a stale record to KernelBuildPath, whose "
+                                    "device asserts and unbounded parent walk can trap or hang a shared GPU; path "
+                                    "costs are reported against the BFS and FP64 Dijkstra optima instead",
             "e2e_step_ms_over_many_frames": p99_long,
-            "batched_over_plain": (e2e_value / plain["value"]) if plain else None,
+            "e2e_attribution": attribution(wall, parts),
             "roofline": {"bound": "hbm", "kernel": "k_search", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": traffic_src,
@@ -649,9 +846,14 @@ def bench_b200(args):
                          "algorithmic_bytes_per_step": statistics.mean(ab)},
             "roofline_issue": issue_roofline(st_sum["rounds"], sum(search_ms), ipr, ipr_src, clocks.get("sm_mhz"),
                                              sms),
+            "mover": {"maze_frames": moving, "cfg2": cfg2},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "path queries/s", "h2d_bytes_per_step": 16 * A + 4,
-                    "d2h_bytes_per_step": 12 * A + 64 + 8 * 8, "p99_step_ms": pct(wall, 99),
+            # per frame: target points to the device point location (8 B) and
+            # the located triangles back (4 B), dirty target records (16 B)
+            # and dt up; positions (8 B) and states (4 B), counters and
+            # statistics back
+            "e2e": {"value": e2e_value, "unit": "path queries/s", "h2d_bytes_per_step": 24 * A + 4,
+                    "d2h_bytes_per_step": 16 * A + 64 + 8 * 9, "p99_step_ms": pct(wall, 99),
                     "p50_step_ms": pct(wall, 50)},
             "gpu_launches": launches,
             "clocks": clocks,
@@ -668,42 +870,48 @@ def bench_b200(args):
 # ---------------------------------------------------------- reference arm --
 
 def bench_reference(args):
+    """The reference has no CPU implementation of the step (PathFinderCPU.h is
+    unused and a different algorithm), so this arm times its C++ restatement
+    in oracle/ on all host cores, on the GPU arm's workload and search shape.
+    Nothing here loads the product library: the navmesh comes from the
+    oracle's own build (the reference's CDT call sequence) and points are
+    located by the oracle."""
     ws, rank, local = dist_env()
     if rank != 0:
         return
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
-    import gmapf_b200 as G
-    from gmapf_b200 import scenarios as S
-    T, C, A = args.threads_per_agent, args.queue_capacity, args.agents
-    scn = S.cfg3(cells=args.cells, seed=3, agents=A, threads_per_agent=T, queue_capacity=C)
-    g = G.GMAPF()
-    g.Init(G.make_config(4, scn.radius, scn.speed, 4, T, C))
-    S.build_map(g, scn)
-    om = O.OMap(g.map_nodes())
-    rng = np.random.default_rng(1003)
+    from gmapf_b200 import scenarios as S  # the seeded scenario generator only (pure numpy)
+    A = args.agents
+    T, C = headline_shape(args)
+    seed = 3
+    scn = S.cfg3(cells=args.cells, seed=seed, agents=A, threads_per_agent=T, queue_capacity=C)
+    tri, nbr = O.navmesh(scn.size, scn.obstacles)
+    om = O.OMap(tri=tri, nbr=nbr)
+    # the GPU arm's frames: agents at seeded free points, every frame a fresh
+    # set of free-point targets from the same generator
+    rng = np.random.default_rng(1000 + scn.seed)
+    starts = om.locate_batch(om.free_points(scn.size, A, rng))
     threads = os.cpu_count() or 1
-    sample = args.ref_sample
+    sample = min(args.ref_sample, A)
     times, qs = [], []
     for k in range(args.warmup + args.steps):
-        s = g.locate(S.free_points(g, scn, sample, rng))
-        t = g.locate(S.free_points(g, scn, sample, rng))
+        targets = om.locate_batch(om.free_points(scn.size, A, rng))
         t0 = time.perf_counter()
-        om.search_batch(s, t, T, C, threads=threads, path_stride=0)
+        om.search_batch(starts[:sample], targets[:sample], T, C, threads=threads, path_stride=0)
         dt = time.perf_counter() - t0
         if k >= args.warmup:
             times.append(dt)
             qs.append(sample)
     value = sum(qs) / sum(times)
-    desc = (f"{sample} queries per step of the {A}-agent frame (uniform free-space starts/targets, same maze, "
-            f"T={T}, C={C}); the reference has no CPU step, so this is its C++ restatement in oracle/")
+    desc = (f"the first {sample} agents' queries of each {A}-agent full-retarget frame (same maze, starts and "
+            f"targets as the GPU arm's frames, T={T}, C={C}); the reference has no CPU step, so this is its C++ "
+            f"restatement in oracle/, {threads} host threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path queries/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i32",
             "data": "synthetic: seeded randomized-DFS maze, uniform free-space starts and targets",
-            "config": {"workload": f"maze {args.cells}x{args.cells} cells on 4000x4000, {A} agents, all "
-                                   f"retargeted every frame", "triangles": g.node_count,
-                       "threads_per_agent": T, "queue_capacity": C, "parallelism": "host threads"},
+            "config": workload_config(args, len(tri), A, T, C),
             "cpu_baseline": {"value": value, "unit": "path queries/s", "cores": threads, "kind": "port",
                              "sample": desc},
             "e2e": {"value": value, "unit": "path queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -790,10 +998,20 @@ def main():
     ap.add_argument("--queue-capacity", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=2048)
     ap.add_argument("--ref-sample", type=int, default=2048)
+    ap.add_argument("--shape", default="", metavar="T,C",
+                    help="headline search shape of both arms (default: the autotuner's pick for the maze)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--quality-sample", type=int, default=128, help="agents whose paths are compared with BFS/Dijkstra")
     ap.add_argument("--no-autotune", action="store_true", help="batched form at the Config's T and C")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-longest", dest="longest", action="store_false",
+                    help="skip timing the frame's slowest search alone")
+    ap.add_argument("--mover-frames", type=int, default=30,
+                    help="frames with every agent walking its path after the full-retarget frames (0: off)")
+    ap.add_argument("--cfg2-steps", type=int, default=1000,
+                    help="steps of the 2,048-agent configuration, retargets every 100 (0: off)")
+    ap.add_argument("--p99-frames-secondary", type=int, default=30,
+                    help="host-API frames of the secondary maze for its p50/p99")
     ap.add_argument("--profile-search", default="", metavar="CELLS,T,C,VM,QUERIES",
                     help="profiling run: one batch search on the CELLS maze (no bench line)")
     ap.add_argument("--profile-budget-mb", type=int, default=0, help="search-state cap of --profile-search")
