@@ -147,10 +147,21 @@ __device__ __forceinline__ void ring_complete(const SearchParams& p, int slot_ro
 __host__ __device__ __forceinline__ size_t search_queue_words(int C, int T) {
     return ((size_t)kEntryWords * C * T + 3) & ~(size_t)3;
 }
-// the round's frontier (3T entries of 3 words) and, for T >= 16, the owner
-// lane of each of the 3T compacted candidates
+// Words of a frontier entry: the queue key (F, G<<1|dir, id) and, for
+// T >= 16, the claimed node's neighbour ids and degree (the first 16 bytes of
+// its SearchRow), fetched while its claim is checked.  Nearly every round
+// pops only nodes claimed in the round before (a search's queues hold few
+// entries better than its newest ones), so the node a lane expands next
+// usually arrives with its neighbours, and the round needs one dependent
+// global access (the claim check) instead of two (its row, then the claim
+// check).  Ring entries stay three words: a node popped from a ring loads
+// its row at the start of the round.
+__host__ __device__ constexpr int frontier_entry_words(int T) { return T >= 16 ? 7 : kEntryWords; }
+
+// the round's frontier (3T entries) and, for T >= 16, the owner lane of each
+// of the 3T compacted candidates
 __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
-    return ((size_t)kEntryWords * 3 * T + (T >= 16 ? 3 * (size_t)T : 0) + 3) & ~(size_t)3;
+    return ((size_t)frontier_entry_words(T) * 3 * T + (T >= 16 ? 3 * (size_t)T : 0) + 3) & ~(size_t)3;
 }
 
 
@@ -257,6 +268,8 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
         // run while the next round's loads are in flight.
         int qbeg = 0, qsize = 0;
         int uid = -1, ugd = 0;
+        int4 urow = make_int4(-1, -1, -1, 0);  // T >= 16: the selected node's row ids and degree, when carried
+        bool ucar = false;                      // urow holds them (the node came from the last frontier)
         float tF = 0.f;
         int tgd = 0, tid = -1;
         bool pop_tail = false;
@@ -293,7 +306,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             // thread index: visited state, the lowest fresh thread of a node
             // claims it, the first conflicting thread is the meeting pair.
             auto resolve = [&](bool valid, int cu, int cgdu, int n, float cx, float cy, const int4& ra,
-                               const int4& rb, int2 cst, bool later_pass) {
+                               const int4& rb, int2 cst, bool later_pass, const int4& rn) {
                 const int du = cgdu & 1;
                 const int ngd = (((cgdu >> 1) + 1) << 1) | du;
                 bool prev = false;
@@ -354,6 +367,12 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     fr[idx] = __float_as_int(F);
                     fr[3 * T + idx] = ngd;
                     fr[6 * T + idx] = n;
+                    if constexpr (T >= 16) {  // the node's row ids and degree travel with it
+                        fr[9 * T + idx] = rn.x;
+                        fr[12 * T + idx] = rn.y;
+                        fr[15 * T + idx] = rn.z;
+                        fr[18 * T + idx] = rn.w;
+                    }
                     if (BMV) bm_set<SMEMV>(bm, n, du);
                     // ancestors 1..5 of n = ancestors 0..4 of the popped node
                     st_rec(rec + n, ep, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
@@ -409,12 +428,12 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     if (VM == 3 && valid) cst.x = (int)__ldcg(bm + (n >> 4));
                 }
                 deferred_queue_work();
-                resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, false);
+                resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, false, make_int4(0, 0, 0, 0));
             } else {
                 // compacted candidates: slot-major (slot 0 of every expanding lane,
                 // then slot 1, then slot 2) -- usually one pass of at most 32
                 int4 r0 = make_int4(-1, -1, -1, 0);
-                if (idu >= 0) r0 = __ldg(reinterpret_cast<const int4*>(p.rows + idu));
+                if (idu >= 0) r0 = ucar ? urow : __ldg(reinterpret_cast<const int4*>(p.rows + idu));
                 deferred_queue_work();
                 const unsigned b0 = __ballot_sync(kFull, idu >= 0 && r0.w > 0);
                 const unsigned b1 = __ballot_sync(kFull, idu >= 0 && r0.w > 1);
@@ -426,7 +445,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 const int n0 = __popc(b0), n1 = __popc(b1), total = n0 + n1 + __popc(b2);
                 // each owner writes its lane at its candidates' compacted positions
                 // (a ballot rank is one popc; the inverse, the n-th set bit, is not)
-                int* oix = fr + 9 * T;
+                int* oix = fr + 21 * T;
                 if (idu >= 0) {
                     if (r0.w > 0) oix[__popc(b0 & lt_mask)] = lane;
                     if (r0.w > 1) oix[n0 + __popc(b1 & lt_mask)] = lane;
@@ -448,6 +467,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     float cx = 0.f, cy = 0.f;
                     int4 ra = make_int4(0, 0, -1, -1), rb = make_int4(-1, -1, -1, -1);
                     int2 cst = make_int2(0, 0);
+                    int4 rn = make_int4(-1, -1, -1, 0);
                     if (valid) {
                         const float2 cc = __ldg(reinterpret_cast<const float2*>(&p.rows[cu].x0) + sl);
                         ld_rec(rec + cu, ra, rb);
@@ -455,8 +475,9 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                         cy = cc.y;
                         if (VM == 2) cst = ld_state(rec + n);
                         if (VM == 3) cst.x = (int)__ldcg(bm + (n >> 4));
+                        rn = __ldg(reinterpret_cast<const int4*>(p.rows + n));  // in flight with the claim check
                     }
-                    resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, base > 0);
+                    resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, base > 0, rn);
                 }
             }
             claims += (unsigned)nwin;
@@ -515,6 +536,13 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 uid = have ? bi : -1;
                 ugd = bg;
                 pop_tail = have && best < 0;  // otherwise the ring is untouched by the pop
+                if constexpr (T >= 16) {
+                    ucar = have && best >= 0;
+                    if (ucar) {
+                        const int i = lane + best * T;
+                        urow = make_int4(fr[9 * T + i], fr[12 * T + i], fr[15 * T + i], fr[18 * T + i]);
+                    }
+                }
 #pragma unroll
                 for (int j = 0; j < 3; j++) pv[j] = pv[j] && j != best;  // the rest waits for insertion
                 if (!__any_sync(kFull, uid >= 0))

@@ -5,12 +5,17 @@ compiled for the host from the reference sources by oracle/ref/build_ref.sh)
 on seeded inputs and stores inputs and outputs as JSON next to this script:
 
   ref_queue.json     bounded-queue push/pop sequences (CuQueue.h:33-70)
+  ref_queue_ties.json  the same with many equal F keys (and distinct G and
+                     ids): the reference orders equal F first-in first-out,
+                     the oracle by (G, id); these cases record the
+                     reference's own order where the two differ
   ref_geometry.json  centroids (src/GMAPF.cu:215), TryGetNodeIdx, IsInNode,
                      GetDistSqr (CuNodesMap.h) and GetRotated(10) (V2Float.h:39-47)
                      on the cfg1, zigzag and a cfg2-shaped navmesh
 
-Queue keys are distinct, so the reference's FIFO order for equal F and the
-oracle's (F, G, id) order cannot differ on them.  Needs the reference tree
+In ref_queue.json the queue keys are distinct, so the reference's FIFO order
+for equal F and the oracle's (F, G, id) order cannot differ on them;
+ref_queue_ties.json is where they can.  Needs the reference tree
 (this script is run where it is mounted; the JSON files travel instead).
 """
 from __future__ import annotations
@@ -67,6 +72,39 @@ def queue_cases(rng):
     return cases
 
 
+def queue_tie_cases(rng):
+    """F drawn from a handful of values, so most pushes tie with queued items;
+    G and ids distinct.  The reference's Push ignores G (it compares F only)."""
+    cases = []
+    for k in range(40):
+        cap = int(rng.choice([2, 3, 4, 6, 8, 16]))
+        nops = int(rng.integers(10, 90))
+        pushes = int(nops * 0.7) + 1
+        F = rng.choice(np.float32([1.5, 2.0, 2.5, 7.0, 9.25])[:int(rng.integers(2, 6))], pushes).astype(np.float32)
+        G = rng.permutation(1000)[:pushes].astype(np.int32)
+        ids = rng.permutation(100000)[:pushes].astype(np.int32)
+        ops, pi = [], 0
+        for _ in range(nops):
+            if pi < pushes and rng.random() < 0.65:
+                ops.append(1)
+                pi += 1
+            else:
+                ops.append(0)
+        lines = [f"Q {cap} {len(ops)}"]
+        j = 0
+        for o in ops:
+            if o == 1:
+                lines.append(f"u {float(F[j]):.9g} {int(ids[j])}")
+                j += 1
+            else:
+                lines.append("o")
+        out = run("\n".join(lines) + "\n")[0]
+        popped, final = out[1:].split("|")
+        cases.append({"cap": cap, "ops": ops, "F": f32s(F[:j]), "G": G[:j].tolist(), "ids": ids[:j].tolist(),
+                      "popped": [int(v) for v in popped.split()], "final": [int(v) for v in final.split()]})
+    return cases
+
+
 def geometry_case(name, nodes, rng):
     tri = np.concatenate([nodes["P1"], nodes["P2"], nodes["P3"]], 1).astype(np.float32)
     nbr = nodes["NeibsIdx"].astype(np.int32)
@@ -111,6 +149,8 @@ def main():
     from gmapf_b200 import GMAPF, make_config
     rng = np.random.default_rng(20261203)
     (HERE / "ref_queue.json").write_text(json.dumps({"cases": queue_cases(rng)}))
+    # drawn from their own generator, so that the files above stay as they were
+    (HERE / "ref_queue_ties.json").write_text(json.dumps({"cases": queue_tie_cases(np.random.default_rng(77))}))
     geo = []
     for scn in [S.cfg1(), S.zigzag(), S.cfg2()]:
         g = GMAPF()

@@ -68,3 +68,62 @@ def test_rotation_constants_match_reference(geo_maps):
         ref = np.asarray(m["rotated_bits"], np.uint32).view(np.float32).reshape(-1, 2)
         ulp = np.spacing(np.abs(ref).max(axis=1, keepdims=True).astype(np.float32))
         assert np.all(np.abs(np.stack([rx, ry], 1) - ref) <= 2 * ulp)
+
+
+def bounded_queue(ops, F, G, ids, cap, key):
+    """A bounded queue kept in descending key order, popped at the minimum:
+    the reference's CuQueue (include/gmapf/misc/CuQueue.h:33-70) when `key`
+    is F alone (an item goes after every queued item with a larger key, so
+    equal keys leave first-in first-out; a full queue drops an item whose key
+    is not below the maximum and otherwise evicts the front, the newest of the
+    maximal keys), the oracle's order when `key` is (F, G, id)."""
+    data, popped, j = [], [], 0
+    for o in ops:
+        if o == 1:
+            it = (key(F[j], G[j], ids[j]), ids[j])
+            j += 1
+            idx = -1
+            for i in range(len(data) - 1, -1, -1):
+                if it[0] < data[i][0]:
+                    idx = i
+                    break
+            if len(data) < cap:
+                data.insert(idx + 1, it)
+            elif idx != -1:
+                data.pop(0)
+                data.insert(idx, it)
+        else:
+            popped.append(data.pop()[1] if data else -1)
+    return popped, [x[1] for x in reversed(data)]
+
+
+@pytest.fixture(scope="module")
+def tie_cases():
+    return json.loads((GOLD / "ref_queue_ties.json").read_text())["cases"]
+
+
+def test_reference_orders_equal_F_first_in_first_out(tie_cases):
+    """The reference's own queue on keys with many ties equals the F-only
+    restatement: equal F leave in push order (CuQueue.h:39-44)."""
+    assert len(tie_cases) >= 30
+    for c in tie_cases:
+        got = bounded_queue(c["ops"], c["F"], c["G"], c["ids"], c["cap"], key=lambda f, g, i: np.float32(f))
+        assert got == (c["popped"], c["final"])
+
+
+def test_oracle_departs_from_the_reference_only_on_equal_F(oracle_mod, tie_cases, queue_cases):
+    """The oracle breaks F ties by (G, id) instead of push order.  With
+    distinct F (every ref_queue.json case) both orders agree; with ties they
+    differ exactly as the two restatements do, and only there."""
+    differ = 0
+    for c in tie_cases:
+        popped, final = oracle_mod.queue_sim(c["F"], c["G"], c["ids"], c["ops"], c["cap"])
+        want = bounded_queue(c["ops"], c["F"], c["G"], c["ids"], c["cap"],
+                             key=lambda f, g, i: (np.float32(f), g, i))
+        assert (popped.tolist(), final.tolist()) == want
+        differ += (popped.tolist(), final.tolist()) != (c["popped"], c["final"])
+    assert differ > 0  # the cases do exercise the departure
+    for c in queue_cases:
+        assert len(set(c["F"])) == len(c["F"])
+        assert bounded_queue(c["ops"], c["F"], [0] * len(c["F"]), c["ids"], c["cap"],
+                             key=lambda f, g, i: np.float32(f)) == (c["popped"], c["final"])
