@@ -979,6 +979,31 @@ def profile_search(spec: str, budget_mb: int, timeline: bool):
     g.close()
 
 
+def profile_frames(workload: str, frames: int):
+    """Frames for profilers (ncu -k on the mover kernels), no bench line.
+    workload "cfg2": the 2,048-agent configuration, all agents retargeted at
+    frame 0 and walking after; "maze64": the 64x64-cell maze with 16,384
+    agents, all retargeted at frame 0 and walking after.  Frame 0 carries the
+    searches; frames 1.. move and collide every agent."""
+    import gmapf_b200 as G
+    from gmapf_b200 import scenarios as S
+    if workload == "cfg2":
+        scn, A = S.cfg2(), 2048
+    else:
+        scn, A = S.cfg3(cells=int(workload[4:])), 16384
+    g, starts, rng = S.make_world(scn, agents=A, threads_per_agent=8, queue_capacity=32, profiler=True)
+    g.ManualStart()
+    g.set_targets(np.arange(A, dtype=np.int32), S.free_points(g, scn, A, rng))
+    st = []
+    for k in range(frames):
+        g.AsyncStep(1.0 / 60.0)
+        g.WaitStepEnd()
+        st.append(g.last_stats())
+    print(json.dumps({"workload": workload, "agents": A, "frames": frames,
+                      "moving": [s["moving"] for s in st], "ms_mover": [round(s["ms_mover"], 4) for s in st]}))
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1016,7 +1041,12 @@ def main():
                     help="profiling run: one batch search on the CELLS maze (no bench line)")
     ap.add_argument("--profile-budget-mb", type=int, default=0, help="search-state cap of --profile-search")
     ap.add_argument("--profile-timeline", action="store_true", help="--profile-search: per-request timeline")
+    ap.add_argument("--profile-frames", default="", metavar="cfg2|mazeN",
+                    help="profiling run: frames of the mover workload (no bench line)")
     args = ap.parse_args()
+    if args.profile_frames:
+        profile_frames(args.profile_frames, max(2, args.steps))
+        return
     if args.profile_search:
         profile_search(args.profile_search, args.profile_budget_mb, args.profile_timeline)
         return
