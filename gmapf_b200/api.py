@@ -334,8 +334,11 @@ class GMAPF:
         self._check(self._lib.gmapf_search_shape(self._h, *[C.byref(x) for x in v]))
         return dict(zip(["T", "C", "block_threads", "visited_mode", "slots"], [x.value for x in v]))
 
-    def search_batch(self, starts, targets, path_stride: int):
-        """Independent searches on host buffers (copies inside the call)."""
+    def search_batch(self, starts, targets, path_stride: int, check: bool = True):
+        """Independent searches on host buffers (copies inside the call).
+        check=False returns the outputs and statistics of a call that reported
+        a device-side check (a path longer than its row, say) instead of
+        raising; the status is then in the statistics' "status"."""
         s = _i32(starts)
         t = _i32(targets)
         n = len(s)
@@ -343,9 +346,13 @@ class GMAPF:
         lens = np.empty(n, np.int32)
         paths = np.full((n, path_stride), -1, np.int32)
         st = StepStats()
-        self._check(self._lib.gmapf_search_batch_host(self._h, _ptr(s), _ptr(t), n, _ptr(found), _ptr(lens),
-                                                       _ptr(paths), path_stride, C.byref(st)))
-        return found, lens, paths, st.as_dict()
+        rc = self._lib.gmapf_search_batch_host(self._h, _ptr(s), _ptr(t), n, _ptr(found), _ptr(lens), _ptr(paths),
+                                               path_stride, C.byref(st))
+        if check or rc not in (0, 8):  # 8: GMAPF_E_DEVICE
+            self._check(rc)
+        d = st.as_dict()
+        d["status"] = rc
+        return found, lens, paths, d
 
     def search_batch_device(self, d_starts: int, d_targets: int, n: int, d_found: int, d_lens: int, d_paths: int,
                             path_stride: int) -> dict:
