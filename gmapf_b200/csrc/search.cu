@@ -36,6 +36,13 @@
 //     global memory, sized to stay in L2 and cleared per query; or the
 //     32-byte records themselves, stamped with the query epoch (no clearing
 //     between queries, but one DRAM round trip per round);
+//   - for T >= 16 the expanded node's parent (carried in its frontier entry)
+//     is not a candidate: it is claimed from the same side, so it changes
+//     nothing;
+//   - the items a lane received but did not select are inserted into its
+//     ring at the start of the next round, read from the frontier that is
+//     still in place (no registers held across the round), and the ring's
+//     cached minimum is reloaded only when the ring changed;
 //   - records (G, parent and five further ancestors) are written once per
 //     claimed node, each as one 32-byte access; the path walk reads one
 //     record per six hops; a node's record is read when it is expanded, in
@@ -147,21 +154,16 @@ __device__ __forceinline__ void ring_complete(const SearchParams& p, int slot_ro
 __host__ __device__ __forceinline__ size_t search_queue_words(int C, int T) {
     return ((size_t)kEntryWords * C * T + 3) & ~(size_t)3;
 }
-// Words of a frontier entry: the queue key (F, G<<1|dir, id) and, for
-// T >= 16, the claimed node's neighbour ids and degree (the first 16 bytes of
-// its SearchRow), fetched while its claim is checked.  Nearly every round
-// pops only nodes claimed in the round before (a search's queues hold few
-// entries better than its newest ones), so the node a lane expands next
-// usually arrives with its neighbours, and the round needs one dependent
-// global access (the claim check) instead of two (its row, then the claim
-// check).  Ring entries stay three words: a node popped from a ring loads
-// its row at the start of the round.
-__host__ __device__ constexpr int frontier_entry_words(int T) { return T >= 16 ? 7 : kEntryWords; }
-
-// the round's frontier (3T entries) and, for T >= 16, the owner lane of each
-// of the 3T compacted candidates
+// The round's frontier (3T entries: the queue key (F, G<<1|dir, id) and, for
+// T >= 16, the claimed node's parent) and, for T >= 16, the owner lane of
+// each of the 3T compacted candidates.  A node's parent is claimed from its
+// side, so when the node is expanded the parent can be neither a claim nor a
+// meeting point: for T >= 16 a node that arrives from the last frontier (the
+// usual case: a search's queues hold few entries better than its newest)
+// leaves its parent out of the round's candidates, which shortens the
+// compacted pass without changing any claim, meet or frontier position.
 __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
-    return ((size_t)frontier_entry_words(T) * 3 * T + (T >= 16 ? 3 * (size_t)T : 0) + 3) & ~(size_t)3;
+    return ((size_t)(kEntryWords + (T >= 16 ? 1 : 0)) * 3 * T + (T >= 16 ? 3 * (size_t)T : 0) + 3) & ~(size_t)3;
 }
 
 
@@ -268,15 +270,12 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
         // run while the next round's loads are in flight.
         int qbeg = 0, qsize = 0;
         int uid = -1, ugd = 0;
-        int4 urow = make_int4(-1, -1, -1, 0);  // T >= 16: the selected node's row ids and degree, when carried
-        bool ucar = false;                      // urow holds them (the node came from the last frontier)
+        int upar = -1;  // the selected node's parent when it came from the last frontier (-1: unknown)
         float tF = 0.f;
         int tgd = 0, tid = -1;
         bool pop_tail = false;
         bool pv[3] = {false, false, false};  // received items waiting for insertion
         bool more = false;                   // warp-uniform: the last round claimed more than T nodes
-        float pxF[3] = {0.f, 0.f, 0.f};
-        int pxg[3] = {0, 0, 0}, pxi[3] = {0, 0, 0};
         if (lane < 2) {  // PathFinder.h:168-189: lane 0 seeds the start, lane 1 the target
             const int node = lane == 0 ? start : target;
             const int gd = lane == 0 ? 1 : 0;
@@ -306,7 +305,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             // thread index: visited state, the lowest fresh thread of a node
             // claims it, the first conflicting thread is the meeting pair.
             auto resolve = [&](bool valid, int cu, int cgdu, int n, float cx, float cy, const int4& ra,
-                               const int4& rb, int2 cst, bool later_pass, const int4& rn) {
+                               const int4& rb, int2 cst, bool later_pass) {
                 const int du = cgdu & 1;
                 const int ngd = (((cgdu >> 1) + 1) << 1) | du;
                 bool prev = false;
@@ -367,12 +366,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     fr[idx] = __float_as_int(F);
                     fr[3 * T + idx] = ngd;
                     fr[6 * T + idx] = n;
-                    if constexpr (T >= 16) {  // the node's row ids and degree travel with it
-                        fr[9 * T + idx] = rn.x;
-                        fr[12 * T + idx] = rn.y;
-                        fr[15 * T + idx] = rn.z;
-                        fr[18 * T + idx] = rn.w;
-                    }
+                    if constexpr (T >= 16) fr[9 * T + idx] = cu;  // its parent: same side, never a claim or a meet
                     if (BMV) bm_set<SMEMV>(bm, n, du);
                     // ancestors 1..5 of n = ancestors 0..4 of the popped node
                     st_rec(rec + n, ep, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
@@ -385,13 +379,19 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             // issued before it are still in flight
             auto deferred_queue_work = [&]() {
                 if (lane < T) {
+                    const bool touched = pop_tail || pv[0] || (more && (pv[1] || pv[2]));
                     if (pop_tail) qsize--;
-                    if (pv[0]) ring_push(ring, qbeg, qsize, C - 1, pxF[0], pxg[0], pxi[0]);
+                    // the last round's frontier is still in place: read the items from it
+                    if (pv[0]) ring_push(ring, qbeg, qsize, C - 1, __int_as_float(fr[lane]), fr[3 * T + lane], fr[6 * T + lane]);
                     if (more) {  // items lane + T, lane + 2T exist only when nwin > T
-                        if (pv[1]) ring_push(ring, qbeg, qsize, C - 1, pxF[1], pxg[1], pxi[1]);
-                        if (pv[2]) ring_push(ring, qbeg, qsize, C - 1, pxF[2], pxg[2], pxi[2]);
+                        if (pv[1])
+                            ring_push(ring, qbeg, qsize, C - 1, __int_as_float(fr[lane + T]), fr[4 * T + lane],
+                                      fr[7 * T + lane]);
+                        if (pv[2])
+                            ring_push(ring, qbeg, qsize, C - 1, __int_as_float(fr[lane + 2 * T]), fr[5 * T + lane],
+                                      fr[8 * T + lane]);
                     }
-                    if (qsize > 0) {
+                    if (touched && qsize > 0) {  // an untouched ring keeps its cached minimum
                         const int k = ring.at(qbeg + qsize - 1);
                         const int2 e = ring.fg()[k];
                         tF = __int_as_float(e.x);
@@ -428,16 +428,21 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     if (VM == 3 && valid) cst.x = (int)__ldcg(bm + (n >> 4));
                 }
                 deferred_queue_work();
-                resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, false, make_int4(0, 0, 0, 0));
+                resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, false);
             } else {
                 // compacted candidates: slot-major (slot 0 of every expanding lane,
                 // then slot 1, then slot 2) -- usually one pass of at most 32
                 int4 r0 = make_int4(-1, -1, -1, 0);
-                if (idu >= 0) r0 = ucar ? urow : __ldg(reinterpret_cast<const int4*>(p.rows + idu));
+                if (idu >= 0) r0 = __ldg(reinterpret_cast<const int4*>(p.rows + idu));
                 deferred_queue_work();
-                const unsigned b0 = __ballot_sync(kFull, idu >= 0 && r0.w > 0);
-                const unsigned b1 = __ballot_sync(kFull, idu >= 0 && r0.w > 1);
-                const unsigned b2 = __ballot_sync(kFull, idu >= 0 && r0.w > 2);
+                // the popped node's parent is claimed from its side: it can be
+                // neither a claim nor a meet, so it is left out of the candidates
+                const bool k0 = idu >= 0 && r0.w > 0 && r0.x != upar;
+                const bool k1 = idu >= 0 && r0.w > 1 && r0.y != upar;
+                const bool k2 = idu >= 0 && r0.w > 2 && r0.z != upar;
+                const unsigned b0 = __ballot_sync(kFull, k0);
+                const unsigned b1 = __ballot_sync(kFull, k1);
+                const unsigned b2 = __ballot_sync(kFull, k2);
                 if (idu >= 0) {
                     expansions++;
                     deg_sum += (unsigned)r0.w;
@@ -445,12 +450,10 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 const int n0 = __popc(b0), n1 = __popc(b1), total = n0 + n1 + __popc(b2);
                 // each owner writes its lane at its candidates' compacted positions
                 // (a ballot rank is one popc; the inverse, the n-th set bit, is not)
-                int* oix = fr + 21 * T;
-                if (idu >= 0) {
-                    if (r0.w > 0) oix[__popc(b0 & lt_mask)] = lane;
-                    if (r0.w > 1) oix[n0 + __popc(b1 & lt_mask)] = lane;
-                    if (r0.w > 2) oix[n0 + n1 + __popc(b2 & lt_mask)] = lane;
-                }
+                int* oix = fr + 12 * T;
+                if (k0) oix[__popc(b0 & lt_mask)] = lane;
+                if (k1) oix[n0 + __popc(b1 & lt_mask)] = lane;
+                if (k2) oix[n0 + n1 + __popc(b2 & lt_mask)] = lane;
                 __syncwarp();
                 for (int base = 0; base < total; base += 32) {  // warp-uniform
                     const int t = base + lane;
@@ -467,7 +470,6 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     float cx = 0.f, cy = 0.f;
                     int4 ra = make_int4(0, 0, -1, -1), rb = make_int4(-1, -1, -1, -1);
                     int2 cst = make_int2(0, 0);
-                    int4 rn = make_int4(-1, -1, -1, 0);
                     if (valid) {
                         const float2 cc = __ldg(reinterpret_cast<const float2*>(&p.rows[cu].x0) + sl);
                         ld_rec(rec + cu, ra, rb);
@@ -475,9 +477,8 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                         cy = cc.y;
                         if (VM == 2) cst = ld_state(rec + n);
                         if (VM == 3) cst.x = (int)__ldcg(bm + (n >> 4));
-                        rn = __ldg(reinterpret_cast<const int4*>(p.rows + n));  // in flight with the claim check
                     }
-                    resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, base > 0, rn);
+                    resolve(valid, cu, cgdu, n, cx, cy, ra, rb, cst, base > 0);
                 }
             }
             claims += (unsigned)nwin;
@@ -513,15 +514,14 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     const int i = lane + j * T;
                     pv[j] = lane < T && i < nwin;
                     if (pv[j]) {
-                        pxF[j] = __int_as_float(fr[i]);
-                        pxg[j] = fr[3 * T + i];
-                        pxi[j] = fr[6 * T + i];
-                        if (!have || key_less(pxF[j], pxg[j], pxi[j], bF, bg, bi)) {
+                        const float xF = __int_as_float(fr[i]);
+                        const int xg = fr[3 * T + i], xi = fr[6 * T + i];
+                        if (!have || key_less(xF, xg, xi, bF, bg, bi)) {
                             best = j;
                             have = true;
-                            bF = pxF[j];
-                            bg = pxg[j];
-                            bi = pxi[j];
+                            bF = xF;
+                            bg = xg;
+                            bi = xi;
                         }
                     }
                 };
@@ -536,13 +536,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 uid = have ? bi : -1;
                 ugd = bg;
                 pop_tail = have && best < 0;  // otherwise the ring is untouched by the pop
-                if constexpr (T >= 16) {
-                    ucar = have && best >= 0;
-                    if (ucar) {
-                        const int i = lane + best * T;
-                        urow = make_int4(fr[9 * T + i], fr[12 * T + i], fr[15 * T + i], fr[18 * T + i]);
-                    }
-                }
+                if constexpr (T >= 16) upar = (have && best >= 0) ? fr[9 * T + lane + best * T] : -1;
 #pragma unroll
                 for (int j = 0; j < 3; j++) pv[j] = pv[j] && j != best;  // the rest waits for insertion
                 if (!__any_sync(kFull, uid >= 0))
