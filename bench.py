@@ -166,27 +166,30 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def measured_traffic(cells: int, T: int, C: int, vm: int, queries_per_step: float):
-    """DRAM bytes per search launch from the committed ncu capture
-    (profiles/search_traffic.json, per query, scaled to this frame's
-    queries), or None when no capture matches this workload and shape."""
-    p = ROOT / "profiles" / "search_traffic.json"
+def search_counters(T: int, C: int, vm: int):
+    """The search kernel's per-unit counters for this shape from the committed
+    ncu capture (profiles/search_counters.json): DRAM bytes per claimed node
+    and warp instructions per round, measured on a small case (the 64x64-cell
+    maze, one 16,384-query launch) and applied to the timed frames' own
+    claims and rounds.  None when no capture matches the shape."""
+    p = ROOT / "profiles" / "search_counters.json"
     if not p.exists():
-        return None, None
-    d = json.loads(p.read_text()).get(f"maze{cells}_T{T}_C{C}_vm{vm}")
+        return None
+    return json.loads(p.read_text()).get(f"T{T}_C{C}_vm{vm}")
+
+
+def measured_traffic(T: int, C: int, vm: int, claims_per_step: float):
+    """DRAM bytes per search launch: the capture's bytes per claimed node
+    times this frame's claims (record writes dominate and grow with claims)."""
+    d = search_counters(T, C, vm)
     if not d:
         return None, None
-    return d["bytes_per_query"] * queries_per_step, d["source"]
+    return d["dram_bytes_per_claim"] * claims_per_step, d["source"]
 
 
-def measured_inst_per_round(cells: int, T: int, C: int, vm: int):
-    """Warp instructions per search round from the committed ncu capture of
-    the full frame (profiles/search_issue.json), or None when no capture
-    matches this workload and shape."""
-    p = ROOT / "profiles" / "search_issue.json"
-    if not p.exists():
-        return None, None
-    d = json.loads(p.read_text()).get(f"maze{cells}_T{T}_C{C}_vm{vm}")
+def measured_inst_per_round(T: int, C: int, vm: int):
+    """Warp instructions per search round from the capture, or None."""
+    d = search_counters(T, C, vm)
     if not d:
         return None, None
     return d["inst_per_round"], d["source"]
@@ -734,9 +737,9 @@ def bench_b200(args):
     search_ms = [s["ms_search"] for s in dstats]
     ab = [algorithmic_bytes(s, n_nodes) for s in dstats]
     achieved = sum(ab) / (sum(search_ms) / 1e3) / 1e9
-    traffic, traffic_src = measured_traffic(args.cells, shape["T"], shape["C"], shape["visited_mode"],
-                                            queries / max(1, K))
-    ipr, ipr_src = measured_inst_per_round(args.cells, shape["T"], shape["C"], shape["visited_mode"])
+    traffic, traffic_src = measured_traffic(shape["T"], shape["C"], shape["visited_mode"],
+                                            sum(s["claims"] for s in dstats) / max(1, K))
+    ipr, ipr_src = measured_inst_per_round(shape["T"], shape["C"], shape["visited_mode"])
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
 
     # frames in which every agent walks its path (the mover at the maze scale)

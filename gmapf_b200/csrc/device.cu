@@ -135,8 +135,11 @@ SceneInfo single_scene(const Context& c) {
 }
 
 // Mover constants of one scene (AgentsMover.h:162,222-224) and its agent grid:
-// cells at least 1.0625 collision distances wide and about four agents per
-// cell, at most 2048 per axis; cell ids continue from cell_base.
+// cells at least 1.0625 collision distances wide and about one agent per
+// cell (a scan over the cells is part of every moving frame; the collision
+// pass reads the 3x3 cells around each agent, so the cell size changes only
+// which agents are read, never the result), at most 2048 per axis; cell ids
+// continue from cell_base.
 ScenePar scene_par(const Device& d, const SceneInfo& si, int cell_base) {
     ScenePar p{};
     p.cd = si.radius * 2.5f;
@@ -145,7 +148,7 @@ ScenePar scene_par(const Device& d, const SceneInfo& si, int cell_base) {
     p.speed = si.speed;
     const double w = std::max(1e-3, (double)si.bx1 - si.bx0), h = std::max(1e-3, (double)si.by1 - si.by0);
     double cell = std::max((double)p.cd * 1.0625, 1e-4);
-    cell = std::max(cell, std::sqrt(w * h / std::max(1.0, 4.0 * si.A)));
+    cell = std::max(cell, std::sqrt(w * h / std::max(1.0, (double)si.A)));
     cell = std::max(cell, std::max(w, h) / 2048.0);
     p.ax0 = si.bx0;
     p.ay0 = si.by0;

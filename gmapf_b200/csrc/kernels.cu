@@ -272,31 +272,41 @@ __global__ void k_move_bin(MoverParams p) {
     p.cell_of[i] = cell;
 }
 
-// exclusive scan of the cell histogram, one block
+// exclusive scan of the cell histogram, one block: each thread sums a run of
+// cells, the runs are scanned with warp shuffles (two block barriers), then
+// each thread writes its run's starts
 __global__ void __launch_bounds__(1024) k_cell_scan(MoverParams p) {
     if (*p.mv_count == 0) return;
-    __shared__ int part[1024];
+    __shared__ int wsum[32];
     const int cells = p.cells;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int per = (cells + 1023) / 1024;
     const int b = tid * per, e = min(b + per, cells);
     int s = 0;
     for (int k = b; k < e; k++) s += p.cell_cnt[k];
-    part[tid] = s;
-    __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        int v = (tid >= o) ? part[tid - o] : 0;
-        __syncthreads();
-        part[tid] += v;
-        __syncthreads();
+    int x = s;  // inclusive scan of the runs within the warp
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    int run = (tid == 0) ? 0 : part[tid - 1];
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int v = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        wsum[lane] = v;  // inclusive warp totals
+    }
+    __syncthreads();
+    int run = x - s + (w > 0 ? wsum[w - 1] : 0);
     for (int k = b; k < e; k++) {
         p.cell_start[k] = run;
         p.cell_fill[k] = run;
         run += p.cell_cnt[k];
     }
-    if (tid == 1023) p.cell_start[cells] = part[1023];
+    if (tid == 1023) p.cell_start[cells] = wsum[31];
 }
 
 __global__ void k_scatter(MoverParams p) {
