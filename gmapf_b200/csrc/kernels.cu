@@ -283,7 +283,8 @@ __global__ void __launch_bounds__(1024) k_cell_scan(MoverParams p) {
     const int per = (cells + 1023) / 1024;
     const int b = tid * per, e = min(b + per, cells);
     int s = 0;
-    for (int k = b; k < e; k++) s += p.cell_cnt[k];
+#pragma unroll 8
+    for (int k = b; k < e; k++) s += p.cell_cnt[k];  // unrolled: the loads of a run are in flight together
     int x = s;  // inclusive scan of the runs within the warp
     for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, x, o);
@@ -301,6 +302,7 @@ __global__ void __launch_bounds__(1024) k_cell_scan(MoverParams p) {
     }
     __syncthreads();
     int run = x - s + (w > 0 ? wsum[w - 1] : 0);
+#pragma unroll 8
     for (int k = b; k < e; k++) {
         p.cell_start[k] = run;
         p.cell_fill[k] = run;
