@@ -44,7 +44,10 @@ def load():
         sys.path.insert(0, str(HERE.parent))
         from gmapf_b200 import build as _build  # the build recipe only (where the CDT headers are)
         cdt = _build.cdt_dir()
-        subprocess.run(["make", "-s", "-C", str(HERE)] + ([f"CDT_DIR={cdt}"] if cdt else []), check=True)
+        # a library built with the CDT headers is not replaced by one built
+        # without them (a machine without the reference tree keeps the first)
+        if cdt or not LIB.exists():
+            subprocess.run(["make", "-s", "-C", str(HERE)] + ([f"CDT_DIR={cdt}"] if cdt else []), check=True)
     lib = C.CDLL(str(LIB))
     sig = {
         "orc_map_create": (C.c_void_p, [F, I, C.c_int]),
