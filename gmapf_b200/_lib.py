@@ -170,7 +170,10 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     if build_if_missing and os.environ.get("GMAPF_NO_BUILD") != "1":
         try:
             from . import build as _build
-            if _build.needs_build(LIB_PATH, _build._sources()) and os.path.exists(_build.NVCC):
+            # a library built with the navmesh builder (CDT headers) is not
+            # replaced by one built without them on a machine that lacks them
+            if _build.needs_build(LIB_PATH, _build._sources()) and os.path.exists(_build.NVCC) and \
+                    (_build.cdt_dir() or not LIB_PATH.exists()):
                 _build.build_library()
         except Exception:
             if not LIB_PATH.exists():
