@@ -187,6 +187,21 @@ def measured_traffic(T: int, C: int, vm: int, claims_per_step: float):
     return d["dram_bytes_per_claim"] * claims_per_step, d["source"]
 
 
+def search_side_counters(T: int, C: int, vm: int, rounds: int, search_ms: float) -> dict:
+    """L2 traffic rate (the capture's L2 bytes per round x the timed frames'
+    rounds over their search time), threads per warp instruction and the
+    share of branches whose targets were uniform across the warp, from the
+    same capture; empty when none matches the shape."""
+    d = search_counters(T, C, vm)
+    if not d or not search_ms:
+        return {}
+    out = {"l2_gbs": d["l2_bytes_per_round"] * rounds / (search_ms / 1e3) / 1e9} if "l2_bytes_per_round" in d else {}
+    for k in ("threads_per_warp_instruction", "branch_targets_uniform_pct"):
+        if k in d:
+            out[k] = d[k]
+    return out
+
+
 def measured_inst_per_round(T: int, C: int, vm: int):
     """Warp instructions per search round from the capture, or None."""
     d = search_counters(T, C, vm)
@@ -867,7 +882,9 @@ def bench_b200(args):
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": traffic_src,
                          "search_ms_per_step": statistics.mean(search_ms),
-                         "algorithmic_bytes_per_step": statistics.mean(ab)},
+                         "algorithmic_bytes_per_step": statistics.mean(ab),
+                         **search_side_counters(shape["T"], shape["C"], shape["visited_mode"], st_sum["rounds"],
+                                                sum(search_ms))},
             "roofline_issue": issue_roofline(st_sum["rounds"], sum(search_ms), ipr, ipr_src, clocks.get("sm_mhz"),
                                              sms),
             "mover": {"maze_frames": moving, "cfg2": cfg2},

@@ -111,3 +111,9 @@ def test_oracle_navmesh_equals_fill_map_end(oracle_mod):
         assert np.array_equal(tri, t2) and np.array_equal(nbr, n2), scn.name
         pts = np.random.default_rng(3).uniform(0, scn.size[0], (2000, 2)).astype(np.float32)
         assert np.array_equal(oracle_mod.OMap(tri=tri, nbr=nbr).locate_batch(pts), g.locate(pts))
+
+
+def test_search_side_counters(bench):
+    d = bench.search_side_counters(32, 16, 3, rounds=35_000_000, search_ms=30.0)
+    assert 100 < d["l2_gbs"] < 20000 and 0 < d["threads_per_warp_instruction"] <= 32
+    assert bench.search_side_counters(2, 8, 1, 1, 1.0) == {}
