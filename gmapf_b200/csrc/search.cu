@@ -63,10 +63,9 @@ namespace {
 
 // (F, G, id) lexicographic; gd = G << 1 | dir
 __device__ __forceinline__ bool key_less(float fa, int ga, int ia, float fb, int gb, int ib) {
-    if (fa != fb) return fa < fb;
-    const int Ga = ga >> 1, Gb = gb >> 1;
-    if (Ga != Gb) return Ga < Gb;
-    return ia < ib;
+    // G<<1|dir with the side bit set orders and ties exactly as G does
+    const int Ga = ga | 1, Gb = gb | 1;
+    return fa != fb ? fa < fb : (Ga != Gb ? Ga < Gb : ia < ib);
 }
 
 // A queued node: its key (F, G<<1|dir, id).
@@ -307,7 +306,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             auto resolve = [&](bool valid, int cu, int cgdu, int n, float cx, float cy, const int4& ra,
                                const int4& rb, int2 cst, bool later_pass) {
                 const int du = cgdu & 1;
-                const int ngd = (((cgdu >> 1) + 1) << 1) | du;
+                const int ngd = cgdu + 2;  // (G + 1) << 1 | dir
                 bool prev = false;
                 int pside = 0, pgd = 0, pknown = 0;  // earlier claim: side, G<<1|side if known
                 if (valid) {
@@ -510,20 +509,20 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 float bF = tF;
                 int bg = tgd, bi = tid;
                 more = nwin > T;
+                // branch-free (an absent item reads slot 0 and is ignored):
+                // selects instead of a divergent branch per item, 5% of a round
                 auto take = [&](int j) {
                     const int i = lane + j * T;
                     pv[j] = lane < T && i < nwin;
-                    if (pv[j]) {
-                        const float xF = __int_as_float(fr[i]);
-                        const int xg = fr[3 * T + i], xi = fr[6 * T + i];
-                        if (!have || key_less(xF, xg, xi, bF, bg, bi)) {
-                            best = j;
-                            have = true;
-                            bF = xF;
-                            bg = xg;
-                            bi = xi;
-                        }
-                    }
+                    const int ii = pv[j] ? i : 0;
+                    const float xF = __int_as_float(fr[ii]);
+                    const int xg = fr[3 * T + ii], xi = fr[6 * T + ii];
+                    const bool better = pv[j] && (!have || key_less(xF, xg, xi, bF, bg, bi));
+                    best = better ? j : best;
+                    have = have || better;
+                    bF = better ? xF : bF;
+                    bg = better ? xg : bg;
+                    bi = better ? xi : bi;
                 };
                 take(0);
                 if (more) {
