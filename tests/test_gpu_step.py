@@ -174,3 +174,24 @@ def test_step_ready_tracks_the_running_step(oracle_mod):
     assert g.step_ready()
     ow.step(scn.dt, 8)
     compare(g, ow, 0)
+
+
+def test_collision_neighbour_counter(oracle_mod):
+    """The step statistics count the agents read from the 3x3 grid cells by
+    the collision pass (the mover's per-agent traffic in the bench's
+    roofline): every agent reads at least its own cell's agents, itself
+    included, when anybody moves; nothing is read when nobody moves."""
+    scn = S.cfg2()
+    A = 512
+    g, ow, rng = make_pair(oracle_mod, scn, A)
+    g.set_options(mode=G.MODE_BATCHED)  # defaults; profiler off is fine for the counters
+    retarget(g, ow, scn, np.arange(A), rng)
+    g.AsyncStep(scn.dt)  # searches: nobody is moving yet
+    g.WaitStepEnd()
+    st = g.last_stats()
+    assert st["moving"] == 0 and st["neighbours"] == 0
+    g.AsyncStep(scn.dt)
+    g.WaitStepEnd()
+    st = g.last_stats()
+    assert st["moving"] > 0
+    assert A <= st["neighbours"] <= A * A
