@@ -184,7 +184,6 @@ def test_collision_neighbour_counter(oracle_mod):
     scn = S.cfg2()
     A = 512
     g, ow, rng = make_pair(oracle_mod, scn, A)
-    g.set_options(mode=G.MODE_BATCHED)  # defaults; profiler off is fine for the counters
     retarget(g, ow, scn, np.arange(A), rng)
     g.AsyncStep(scn.dt)  # searches: nobody is moving yet
     g.WaitStepEnd()
