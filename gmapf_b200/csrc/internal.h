@@ -15,9 +15,12 @@ namespace gmapf_b200 {
 
 // ------------------------------------------------------------------ device --
 
-// Per-slot visited record of one claimed node, 32 bytes.  `stamp` equals the
-// slot's current query epoch iff the node is claimed by that query, so slots
-// are reused across queries and frames without clearing.  `gd` = G << 1 | dir
+// Per-slot visited record of one claimed node, 32 bytes.  With stamped
+// records (visited placement 2) `stamp` equals the slot's current query epoch
+// iff the node is claimed by that query, so slots are reused across queries
+// and frames without clearing; with a visited bitmap the same word holds the
+// node's jump ancestor (the nearest proper ancestor at a depth that is a
+// multiple of 256, -1 at the root) for a parallel path walk.  `gd` = G << 1 | dir
 // (dir 1 = reached from the start, PathNode::FromStart).  anc[0] is the
 // parent (PathNode::PrevNodeIdx); anc[k] the (k+1)-th ancestor, so a path
 // walk advances six hops per record read.  One 32-byte sector: it is read

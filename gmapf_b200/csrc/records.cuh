@@ -18,7 +18,7 @@ __device__ __forceinline__ void ld_rec(const Rec* r, int4& a, int4& b) {
                  : "l"(r));
 }
 
-// {stamp, G<<1|dir, ancestors 1..6}
+// {stamp or jump ancestor, G<<1|dir, ancestors 1..6}
 __device__ __forceinline__ void st_rec(Rec* r, unsigned stamp, int gd, int a0, int a1, int a2, int a3, int a4,
                                        int a5) {
     asm volatile("st.global.cg.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(r), "r"((int)stamp), "r"(gd),

@@ -166,6 +166,102 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
 }
 
 
+// Record word 0 in the bitmap placements: the nearest proper ancestor whose
+// depth (G) is a multiple of kJumpDepth, -1 at a search's root.
+constexpr int kJumpDepth = 256;
+
+// Path output: depth d of the start side at out[d - 1] (d >= 1), depth d of
+// the target side at out[gS + gT - d] (d >= 0).
+__device__ __forceinline__ int path_pos(int side, int d, int gS, int gT) {
+    return side == 0 ? d - 1 : gS + gT - d;
+}
+
+// Writes the path nodes at depths dx-1 down to b of one side, reading the
+// records from node x (depth dx) down: six nodes per record.
+__device__ __forceinline__ void walk_segment(const Rec* rec, int n_nodes, int* out, int side, int x, int dx, int b,
+                                             int gS, int gT, int* err) {
+    int g = dx;
+    while (g > b) {
+        if (x < 0 || x >= n_nodes) {
+            atomicOr(err, ERR_BOUNDS);
+            break;
+        }
+        int4 a, c;
+        ld_rec(rec + x, a, c);
+        const int anc[6] = {a.z, a.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            const int d = g - 1 - j;
+            if (d >= b) out[path_pos(side, d, gS, gT)] = anc[j];
+        }
+        x = anc[5];
+        g -= 6;
+    }
+}
+
+// Path walk of one warp.  With jump ancestors (records of the bitmap
+// placements), lanes 0 and 1 first follow each side's jump chain from the
+// meeting node, writing the checkpoints (the path nodes at depths that are
+// multiples of kJumpDepth) to their output positions; then the segments
+// between checkpoints, kJumpDepth hops each, are walked by all lanes at once.
+// A path of g hops per side takes about g / kJumpDepth + kJumpDepth / 6
+// dependent record reads instead of g / 6.  Without jump ancestors (stamped
+// records) lanes 0 and 1 walk their sides from the meeting node.
+template <bool JUMP>
+__device__ __forceinline__ void walk_path(const Rec* rec, int n_nodes, int* out, int mS, int gS, int mT, int gT,
+                                          int lane, int* err) {
+    if (lane == 0 && gS >= 1) out[gS - 1] = mS;
+    if (lane == 1) out[gS] = mT;
+    if constexpr (!JUMP) {
+        if (lane < 2)
+            walk_segment(rec, n_nodes, out, lane, lane == 0 ? mS : mT, lane == 0 ? gS : gT, lane == 0 ? 1 : 0, gS,
+                         gT, err);
+    } else {
+        // checkpoints k*D, k = 1..K of each side: K = (g - 1) / D
+        int kc = 0;
+        bool bad = false;
+        if (lane < 2) {
+            const int g = lane == 0 ? gS : gT;
+            int x = lane == 0 ? mS : mT;
+            kc = g >= 1 ? (g - 1) / kJumpDepth : 0;
+            for (int k = kc; k >= 1; k--) {
+                if (x < 0 || x >= n_nodes) {
+                    bad = true;
+                    break;
+                }
+                x = (int)__ldcg(&rec[x].stamp);  // the nearest ancestor at a multiple of D: depth k*D
+                out[path_pos(lane, k * kJumpDepth, gS, gT)] = x;
+            }
+        }
+        if (__any_sync(kFull, bad)) {
+            if (lane == 0) atomicOr(err, ERR_BOUNDS);
+            return;
+        }
+        const int kS = __shfl_sync(kFull, kc, 0), kT = __shfl_sync(kFull, kc, 1);
+        __syncwarp();  // the checkpoints are written
+        // segment k of a side: k = 0 from the meeting node down to depth kD + 1
+        // (or the side's last depth), k >= 1 from the checkpoint at depth kD
+        const int m = kS + 1 + kT + 1;
+        for (int i = lane; i < m; i += 32) {
+            const int side = i <= kS ? 0 : 1;
+            const int k = side == 0 ? i : i - (kS + 1);
+            const int kk = side == 0 ? kS : kT;
+            const int last = side == 0 ? 1 : 0;
+            int x, dx, b;
+            if (k == 0) {
+                x = side == 0 ? mS : mT;
+                dx = side == 0 ? gS : gT;
+                b = kk >= 1 ? kk * kJumpDepth + 1 : last;
+            } else {
+                dx = k * kJumpDepth;
+                x = out[path_pos(side, dx, gS, gT)];
+                b = k == 1 ? last : (k - 1) * kJumpDepth + 1;
+            }
+            walk_segment(rec, n_nodes, out, side, x, dx, b, gS, gT, err);
+        }
+    }
+}
+
 // VM: visited placement (1 shared-memory bitmap, 2 stamped records, 3 global
 // bitmap).  In modes 1 and 3 a bit set by one thread is seen by the others
 // after the next __syncwarp (bar.warp.sync orders memory among its threads).
@@ -175,6 +271,7 @@ template <int T, int VM>
 __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
     constexpr bool SMEMV = VM == 1;  // bitmap in shared memory
     constexpr bool BMV = VM != 2;    // visited state in a bitmap (shared or global)
+    constexpr bool JUMP = VM != 2;   // record word 0: the jump ancestor (else the query stamp)
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;                 // warp in block
@@ -280,7 +377,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             const int gd = lane == 0 ? 1 : 0;
             uid = node;
             ugd = gd;
-            st_rec(rec + node, ep, gd, -1, -1, -1, -1, -1, -1);
+            st_rec(rec + node, JUMP ? 0xffffffffu : ep, gd, -1, -1, -1, -1, -1, -1);
             if (BMV) bm_set<SMEMV>(bm, node, gd);
         }
         (void)f0;  // the seeds' F never takes part in a comparison: each seed is alone in its queue
@@ -368,7 +465,10 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                     if constexpr (T >= 16) fr[9 * T + idx] = cu;  // its parent: same side, never a claim or a meet
                     if (BMV) bm_set<SMEMV>(bm, n, du);
                     // ancestors 1..5 of n = ancestors 0..4 of the popped node
-                    st_rec(rec + n, ep, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
+                    // the jump ancestor: the parent when its depth is a multiple of
+                    // kJumpDepth, else the parent's jump ancestor (its record word 0)
+                    const unsigned w0 = JUMP ? (((cgdu >> 1) & (kJumpDepth - 1)) == 0 ? (unsigned)cu : (unsigned)ra.x) : ep;
+                    st_rec(rec + n, w0, ngd, cu, ra.z, ra.w, rb.x, rb.y, rb.z);
                 }
                 nwin += __popc(wm);
                 __syncwarp();
@@ -556,39 +656,8 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             const int row = (agent >= 0) ? agent : orow;
             if ((long long)L > p.path_stride) {
                 if (lane == 0) atomicOr(p.err, ERR_PATH_CAP);
-            } else if (lane < 2) {
-                int* out = p.paths + (long long)row * p.path_stride;
-                // lane 0: start side, depths gS..1 at positions gS-1..0
-                // lane 1: target side, depths gT..0 at positions gS..gS+gT
-                int x = lane == 0 ? mS : mT;
-                int g = lane == 0 ? gS : gT;
-                const int stop = lane == 0 ? 1 : 0;
-                if (lane == 0) {
-                    if (g >= 1) out[g - 1] = x;
-                } else {
-                    out[gS] = x;
-                }
-                while (g > stop) {
-                    if (x < 0 || x >= n_nodes) {
-                        atomicOr(p.err, ERR_BOUNDS);
-                        break;
-                    }
-                    int4 a, b;
-                    ld_rec(rec + x, a, b);
-                    const int anc[6] = {a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-                    for (int j = 0; j < 6; j++) {
-                        const int d = g - 1 - j;
-                        if (d >= stop) {
-                            if (lane == 0)
-                                out[d - 1] = anc[j];
-                            else
-                                out[gS + gT - d] = anc[j];
-                        }
-                    }
-                    x = anc[5];
-                    g -= 6;
-                }
+            } else {
+                walk_path<JUMP>(rec, n_nodes, p.paths + (long long)row * p.path_stride, mS, gS, mT, gT, lane, p.err);
             }
         }
         __syncwarp();
