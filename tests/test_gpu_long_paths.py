@@ -48,7 +48,7 @@ def queries():
     return np.array(s, np.int32), np.array(t, np.int32)
 
 
-@pytest.mark.parametrize("T,Cap", [(32, 16), (8, 32)])
+@pytest.mark.parametrize("T,Cap", [(32, 16), (16, 16), (8, 32)])
 @pytest.mark.parametrize("vm", [1, 2, 3])
 def test_long_corridor_paths(oracle_mod, T, Cap, vm):
     nodes = corridor(N)
