@@ -874,7 +874,9 @@ def bench_b200(args):
             "path_quality": quality,
             "reference_cuda_build": "not run: its claim race can feed a stale record to KernelBuildPath, whose "
                                     "device asserts and unbounded parent walk can trap or hang a shared GPU; path "
-                                    "costs are reported against the BFS and FP64 Dijkstra optima instead",
+                                    "costs are reported against the BFS and FP64 Dijkstra optima instead, and "
+                                    "against its own queue and claim orders emulated on the CPU "
+                                    "(oracle/reference_order_paths.py)",
             "e2e_step_ms_over_many_frames": p99_long,
             "e2e_attribution": attribution(wall, parts),
             "e2e_sequential": e2e_seq,

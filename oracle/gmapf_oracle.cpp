@@ -178,17 +178,23 @@ inline bool qless(const QItem& a, const QItem& b) {
 }
 
 /* Bounded queue kept in descending key order, minimum at the back, as the
- * reference's CuQueue (CuQueue.h:33-70). */
+ * reference's CuQueue (CuQueue.h:33-70).  fifo: the reference's own key, F
+ * alone: a new item goes after every queued item with a larger F, so equal F
+ * leave first in first out and a full queue evicts the newest of the maximal
+ * F (CuQueue.h:39-63); otherwise the (F, G, id) order the kernels use. */
 struct BQueue {
     std::vector<QItem> d;
     int cap = 0;
-    void reset(int c) { d.clear(); cap = c; d.reserve(c + 1); }
+    bool fifo = false;
+    void reset(int c, bool f = false) { d.clear(); cap = c; fifo = f; d.reserve(c + 1); }
     bool empty() const { return d.empty(); }
     QItem pop() { QItem x = d.back(); d.pop_back(); return x; }
     void push(const QItem& it) {
         /* position: after every element that is greater than `it` */
-        auto pos = std::lower_bound(d.begin(), d.end(), it,
-                                    [](const QItem& a, const QItem& b) { return qless(b, a); });
+        auto pos = fifo ? std::lower_bound(d.begin(), d.end(), it,
+                                           [](const QItem& a, const QItem& b) { return a.F > b.F; })
+                        : std::lower_bound(d.begin(), d.end(), it,
+                                           [](const QItem& a, const QItem& b) { return qless(b, a); });
         if ((int)d.size() < cap) {
             d.insert(pos, it);
             return;
@@ -219,8 +225,27 @@ struct SearchScratch {
     }
 };
 
+/* The reference's own orders, emulated for path-cost comparisons (the
+ * kernels follow the deterministic order): fifo = its queue key (above);
+ * seed != 0 = within each neighbour slot of a round, the expanding lanes in a
+ * seeded random order: the reference's threads take their slots in step but
+ * race inside each claim and frontier append (atomicExch, atomicAdd;
+ * PathFinder.h:198-231), so claims, the meeting pair and frontier positions
+ * follow that order. */
+struct SearchOrder {
+    int fifo = 0;
+    uint64_t seed = 0;
+};
+
+inline uint64_t mix64(uint64_t x) {  /* splitmix64 finaliser */
+    x += 0x9e3779b97f4a7c15ull;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
 int search(const Map& m, int start, int target, int T, int C, float K, SearchScratch& s,
-           std::vector<int>& path, orc_search_stats* st) {
+           std::vector<int>& path, orc_search_stats* st, const SearchOrder& ord = SearchOrder()) {
     s.ensure(m.n, T);
     path.clear();
     if (start == target) return 1; /* already there: found, empty path */
@@ -229,8 +254,10 @@ int search(const Map& m, int start, int target, int T, int C, float K, SearchScr
         s.epoch = 1;
     }
     const uint32_t ep = s.epoch;
-    for (int q = 0; q < T; q++) s.q[q].reset(C);
+    for (int q = 0; q < T; q++) s.q[q].reset(C, ord.fifo != 0);
     orc_search_stats loc{0, 0, 0, 0};
+    uint64_t rng = ord.seed ? mix64(ord.seed ^ ((uint64_t)(uint32_t)start << 32 | (uint32_t)target)) : 0;
+    std::vector<int> cand_q, cand_s;  /* racing order: candidates (lane, slot) in order */
 
     auto claim = [&](int n, int d, int G, int pv) {
         s.stamp[n] = ep;
@@ -263,8 +290,31 @@ int search(const Map& m, int start, int target, int T, int C, float K, SearchScr
         }
         s.frontier.clear();
         bool meet = false;
-        for (int slot = 0; slot < 3; slot++) {
-            for (int q = 0; q < T; q++) {
+        /* candidate order: slot-major, lanes ascending (deterministic) or in a
+         * random order within each slot (Fisher-Yates) */
+        cand_q.clear();
+        cand_s.clear();
+        if (ord.seed) {
+            std::vector<int> lanes;
+            for (int slot = 0; slot < 3; slot++) {
+                lanes.clear();
+                for (int q = 0; q < T; q++)
+                    if (has[q] && slot < m.deg[popped[q].id]) lanes.push_back(q);
+                for (int k = (int)lanes.size() - 1; k > 0; k--) {
+                    rng = mix64(rng);
+                    std::swap(lanes[k], lanes[(int)(rng % (uint64_t)(k + 1))]);
+                }
+                for (int q : lanes) {
+                    cand_q.push_back(q);
+                    cand_s.push_back(slot);
+                }
+            }
+        }
+        const int ncand = ord.seed ? (int)cand_q.size() : 3 * T;
+        for (int c = 0; c < ncand; c++) {
+            {
+                const int q = ord.seed ? cand_q[c] : c % T;
+                const int slot = ord.seed ? cand_s[c] : c / T;
                 if (!has[q]) continue;
                 const QItem& u = popped[q];
                 if (slot >= m.deg[u.id]) continue;
@@ -585,6 +635,56 @@ int orc_search_batch(const orc_map* m, const int* starts, const int* targets, in
         }
     }
     return overflow ? -1 : 0;
+}
+
+int orc_search_batch_order(const orc_map* m, const int* starts, const int* targets, int n, int T,
+                           int C, float K, int fifo, unsigned long long seed, int* found, int* lens,
+                           int* paths_out, int path_stride, orc_search_stats* st_total, int threads) {
+    threads = std::max(1, threads);
+    SearchOrder ord;
+    ord.fifo = fifo;
+    ord.seed = seed;
+    std::vector<SearchScratch> scratch(threads);
+    std::vector<orc_search_stats> st(threads, orc_search_stats{0, 0, 0, 0});
+    std::atomic<int> overflow{0};
+    parallel_for(n, threads, [&](int i, int t) {
+        std::vector<int> p;
+        found[i] = search(*m, starts[i], targets[i], T, C, K, scratch[t], p, &st[t], ord);
+        lens[i] = (int)p.size();
+        if (paths_out) {
+            if ((int)p.size() > path_stride) overflow = 1;
+            else std::copy(p.begin(), p.end(), paths_out + (size_t)i * path_stride);
+        }
+    });
+    if (st_total) {
+        for (auto& x : st) {
+            st_total->rounds += x.rounds;
+            st_total->expansions += x.expansions;
+            st_total->claims += x.claims;
+            st_total->deg_sum += x.deg_sum;
+        }
+    }
+    return overflow ? -1 : 0;
+}
+
+int orc_queue_sim_order(const float* F, const int* G, const int* id, int n_items, const int* ops,
+                        int n_ops, int C, int fifo, int* out_popped, int* out_final) {
+    BQueue q;
+    q.reset(C, fifo != 0);
+    int next = 0, npop = 0;
+    for (int k = 0; k < n_ops; k++) {
+        if (ops[k] == 1) {
+            if (next < n_items) {
+                q.push(QItem{F[next], G[next], id[next], 0});
+                next++;
+            }
+        } else {
+            out_popped[npop++] = q.empty() ? -1 : q.pop().id;
+        }
+    }
+    int sz = (int)q.d.size();
+    for (int i = 0; i < sz; i++) out_final[i] = q.d[sz - 1 - i].id;
+    return sz;
 }
 
 int orc_queue_sim(const float* F, const int* G, const int* id, int n_items, const int* ops,

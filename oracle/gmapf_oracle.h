@@ -84,6 +84,22 @@ int orc_search_batch(const orc_map* m, const int* starts, const int* targets, in
 int orc_queue_sim(const float* F, const int* G, const int* id, int n_items,
                   const int* ops, int n_ops, int C, int* out_popped, int* out_final);
 
+/* The same searches with the reference's own orders emulated, for path-cost
+ * comparisons: fifo = 1 orders each queue by F alone, equal F first in first
+ * out (CuQueue.h:39-63); seed != 0 takes the lanes of each neighbour slot of
+ * a round in a seeded random order, as the reference's threads race inside
+ * each claim and frontier append (PathFinder.h:198-231).  fifo = 0 and
+ * seed = 0 is orc_search_batch. */
+int orc_search_batch_order(const orc_map* m, const int* starts, const int* targets, int n,
+                           int T, int C, float K, int fifo, unsigned long long seed, int* found,
+                           int* lens, int* paths_out, int path_stride, orc_search_stats* st_total,
+                           int threads);
+
+/* orc_queue_sim with the reference's own key when fifo = 1 (F alone, equal F
+ * first in first out). */
+int orc_queue_sim_order(const float* F, const int* G, const int* id, int n_items,
+                        const int* ops, int n_ops, int C, int fifo, int* out_popped, int* out_final);
+
 /* Cost references */
 int orc_bfs_hops(const orc_map* m, int s, int t);
 double orc_dijkstra_len(const orc_map* m, int s, int t);

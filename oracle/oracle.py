@@ -65,6 +65,9 @@ def load():
         "orc_search_batch": (C.c_int, [C.c_void_p, I, I, C.c_int, C.c_int, C.c_int, C.c_float, I, I, I, C.c_int,
                                        C.POINTER(SearchStats), C.c_int]),
         "orc_queue_sim": (C.c_int, [F, I, I, C.c_int, I, C.c_int, C.c_int, I, I]),
+        "orc_search_batch_order": (C.c_int, [C.c_void_p, I, I, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
+                                             C.c_ulonglong, I, I, I, C.c_int, C.POINTER(SearchStats), C.c_int]),
+        "orc_queue_sim_order": (C.c_int, [F, I, I, C.c_int, I, C.c_int, C.c_int, C.c_int, I, I]),
         "orc_bfs_hops": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
         "orc_dijkstra_len": (C.c_double, [C.c_void_p, C.c_int, C.c_int]),
         "orc_world_set_smoothing": (None, [C.c_void_p, C.c_int]),
@@ -169,8 +172,11 @@ class OMap:
                                 C.byref(st))
         return f, path[:L.value].copy(), st.as_dict()
 
-    def search_batch(self, starts, targets, T, Cap, K=1.0, threads=None, path_stride=None):
-        """path_stride=0: lengths and counters only, no path rows."""
+    def search_batch(self, starts, targets, T, Cap, K=1.0, threads=None, path_stride=None, order=None):
+        """path_stride=0: lengths and counters only, no path rows.  order=(fifo,
+        seed) emulates the reference's own orders (orc_search_batch_order):
+        fifo=1 its queue key, F alone with equal F first in first out; seed != 0
+        the lanes of each neighbour slot of a round in a seeded random order."""
         s = np.ascontiguousarray(starts, np.int32)
         t = np.ascontiguousarray(targets, np.int32)
         n = len(s)
@@ -179,9 +185,14 @@ class OMap:
         lens = np.empty(n, np.int32)
         paths = np.full((n, stride), -1, np.int32) if stride > 0 else None
         st = SearchStats()
-        rc = self.lib.orc_search_batch(self.h, _p(s), _p(t), n, int(T), int(Cap), float(K), _p(found), _p(lens),
-                                       _p(paths) if paths is not None else None, stride, C.byref(st),
-                                       int(threads or os.cpu_count() or 1))
+        nthr = int(threads or os.cpu_count() or 1)
+        if order is None:
+            rc = self.lib.orc_search_batch(self.h, _p(s), _p(t), n, int(T), int(Cap), float(K), _p(found), _p(lens),
+                                           _p(paths) if paths is not None else None, stride, C.byref(st), nthr)
+        else:
+            rc = self.lib.orc_search_batch_order(self.h, _p(s), _p(t), n, int(T), int(Cap), float(K), int(order[0]),
+                                                 int(order[1]), _p(found), _p(lens),
+                                                 _p(paths) if paths is not None else None, stride, C.byref(st), nthr)
         if rc != 0:
             raise RuntimeError("oracle path row too small")
         return found, lens, paths, st.as_dict()
@@ -197,7 +208,7 @@ class OMap:
         return self.lib.orc_path_len(self.h, int(s), _p(p), len(p))
 
 
-def queue_sim(F_, G_, ids, ops, cap):
+def queue_sim(F_, G_, ids, ops, cap, fifo=False):
     lib = load()
     F_ = np.ascontiguousarray(F_, np.float32)
     G_ = np.ascontiguousarray(G_, np.int32)
@@ -205,8 +216,12 @@ def queue_sim(F_, G_, ids, ops, cap):
     ops = np.ascontiguousarray(ops, np.int32)
     popped = np.full(len(ops), -2, np.int32)
     final = np.full(max(1, cap), -2, np.int32)
-    k = lib.orc_queue_sim(_p(F_, C.c_float), _p(G_), _p(ids), len(F_), _p(ops), len(ops), int(cap), _p(popped),
-                          _p(final))
+    if fifo:
+        k = lib.orc_queue_sim_order(_p(F_, C.c_float), _p(G_), _p(ids), len(F_), _p(ops), len(ops), int(cap), 1,
+                                    _p(popped), _p(final))
+    else:
+        k = lib.orc_queue_sim(_p(F_, C.c_float), _p(G_), _p(ids), len(F_), _p(ops), len(ops), int(cap), _p(popped),
+                              _p(final))
     npop = int((np.asarray(ops) == 0).sum())
     return popped[:npop].copy(), final[:k].copy()
 

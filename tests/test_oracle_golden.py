@@ -127,3 +127,14 @@ def test_oracle_departs_from_the_reference_only_on_equal_F(oracle_mod, tie_cases
         assert len(set(c["F"])) == len(c["F"])
         assert bounded_queue(c["ops"], c["F"], [0] * len(c["F"]), c["ids"], c["cap"],
                              key=lambda f, g, i: np.float32(f)) == (c["popped"], c["final"])
+
+
+def test_emulated_reference_queue_is_the_reference(oracle_mod, tie_cases, queue_cases):
+    """The oracle's emulation of the reference's own queue key (F alone, equal
+    F first in first out; orc_queue_sim_order with fifo=1), used only for
+    path-cost comparisons, reproduces the reference's CuQueue on every golden
+    case, ties included."""
+    for c in list(tie_cases) + list(queue_cases):
+        G_ = c.get("G", [0] * len(c["F"]))
+        popped, final = oracle_mod.queue_sim(c["F"], G_, c["ids"], c["ops"], c["cap"], fifo=True)
+        assert (popped.tolist(), final.tolist()) == (c["popped"], c["final"])
