@@ -43,11 +43,13 @@
 //     ring at the start of the next round, read from the frontier that is
 //     still in place (no registers held across the round), and the ring's
 //     cached minimum is reloaded only when the ring changed;
-//   - records (G, parent and five further ancestors) are written once per
-//     claimed node, each as one 32-byte access; the path walk reads one
-//     record per six hops; a node's record is read when it is expanded, in
-//     flight together with its row (T <= 8) or with its neighbours' visited
-//     state (T >= 16);
+//   - records (G, parent and five further ancestors; with a visited bitmap
+//     also the jump ancestor, the nearest ancestor at a depth that is a
+//     multiple of 256) are written once per claimed node, each as one 32-byte
+//     access; the path walk reads one record per six hops, on all lanes at
+//     once between the jump ancestors; a node's record is read when it is
+//     expanded, in flight together with its row (T <= 8) or with its
+//     neighbours' visited state (T >= 16);
 //   - idle warps refill from a device work counter (persistent form) or
 //     stop (plain form).
 #include <cuda_runtime.h>
