@@ -61,10 +61,12 @@ def make_config(agents_max: int, radius: float, speed: float, parallel_agents: i
 
 def make_options(mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0, autotune: bool = False,
                  search_mem_budget: int = 0, order_by_estimate: bool = True, visited_mode: int = 0,
-                 path_smoothing: bool = False, round_limit: int = 0) -> Options:
+                 path_smoothing: int = 0, round_limit: int = 0) -> Options:
+    """path_smoothing: 0 / False off, 1 / True funnel corners, 2 corners one
+    agent radius off the walls."""
     o = Options()
     o.round_limit = round_limit
-    o.path_smoothing = 1 if path_smoothing else 0
+    o.path_smoothing = int(path_smoothing)
     o.device = device
     o.mode = mode
     o.block_threads = block_threads

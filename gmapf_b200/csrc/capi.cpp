@@ -201,6 +201,8 @@ gmapf_status gmapf_set_options(gmapf_ctx* ctx, const gmapf_options* o) {
     if (o->visited_mode < 0 || o->visited_mode > 3)
         return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
     if (o->round_limit < 0) return fail(GMAPF_E_INVALID_ARG, "round_limit must be >= 0 (0: no practical limit)");
+    if (o->path_smoothing < 0 || o->path_smoothing > 2)
+        return fail(GMAPF_E_INVALID_ARG, "path_smoothing must be 0 (off), 1 (funnel corners) or 2 (corners one agent radius off the walls)");
     c.opt = *o;
     if (o->block_threads) c.block_threads = o->block_threads;
     return GMAPF_OK;
@@ -1102,6 +1104,8 @@ gmapf_status gmapf_batch_create(gmapf_ctx* const* scenes, int32_t n, const gmapf
             return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
         if (opt->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
         if (opt->round_limit < 0) return fail(GMAPF_E_INVALID_ARG, "round_limit must be >= 0");
+        if (opt->path_smoothing < 0 || opt->path_smoothing > 2)
+            return fail(GMAPF_E_INVALID_ARG, "path_smoothing must be 0, 1 or 2");
     }
     gmapf_batch* b = new (std::nothrow) gmapf_batch();
     gmapf_ctx* w = new (std::nothrow) gmapf_ctx();

@@ -146,6 +146,7 @@ ScenePar scene_par(const Device& d, const SceneInfo& si, int cell_base) {
     p.cd2 = p.cd * p.cd;
     p.arrive = FLT_EPSILON + si.radius;
     p.speed = si.speed;
+    p.clear = d.clearance ? si.radius : 0.f;
     const double w = std::max(1e-3, (double)si.bx1 - si.bx0), h = std::max(1e-3, (double)si.by1 - si.by0);
     double cell = std::max((double)p.cd * 1.0625, 1e-4);
     cell = std::max(cell, std::sqrt(w * h / std::max(1.0, (double)si.A)));
@@ -450,6 +451,7 @@ int device_start(Context& c, std::string& err) {
         }
     }
     DALLOC(d.paths, (size_t)std::max(1, A) * d.path_stride);
+    d.clearance = c.opt.path_smoothing == 2;
     if (c.opt.path_smoothing) {
         size_t freeb = 0, totalb = 0;
         CK(cudaMemGetInfo(&freeb, &totalb));

@@ -100,6 +100,7 @@ struct ScenePar {
     float cd, cd2;           // collision distance (2.5 r) and its square
     float arrive;            // FLT_EPSILON + r
     float speed;
+    float clear;             // path smoothing 2: portals narrowed by r at both ends (else 0)
     LocateGrid loc;          // this scene's triangles (found ids are global)
 };
 
@@ -273,6 +274,7 @@ struct Device {
     int* agent_scene = nullptr;
     int *scene_abase = nullptr, *scene_P = nullptr, *scene_first = nullptr;
     float2* waypoints = nullptr;  // path smoothing (A x path_stride)
+    bool clearance = false;       // path smoothing 2: corners kept one agent radius off the walls
     // batch API scratch
     int4* breq = nullptr;
     int breq_cap = 0;

@@ -501,10 +501,28 @@ __device__ __forceinline__ float area2(float2 a, float2 b, float2 c) {
 
 __device__ __forceinline__ bool veq(float2 a, float2 b) { return a.x == b.x && a.y == b.y; }
 
+// path smoothing 2: both ends of an edge portal moved inward by c (the agent
+// radius), so that the funnel's corners keep that distance from the walls; a
+// portal no wider than 2c becomes its midpoint
+__device__ __forceinline__ void narrow_portal(float2& l, float2& r, float c) {
+    if (!(c > 0.f)) return;
+    const float dx = GM_FSUB(r.x, l.x), dy = GM_FSUB(r.y, l.y);
+    const float w = GM_FSQRT(GM_FADD(GM_FMUL(dx, dx), GM_FMUL(dy, dy)));
+    if (w > GM_FADD(c, c)) {
+        const float t = GM_FDIV(c, w);
+        const float ox = GM_FMUL(dx, t), oy = GM_FMUL(dy, t);
+        l = make_float2(GM_FADD(l.x, ox), GM_FADD(l.y, oy));
+        r = make_float2(GM_FSUB(r.x, ox), GM_FSUB(r.y, oy));
+    } else {
+        const float mx = GM_FMUL(GM_FADD(l.x, r.x), 0.5f), my = GM_FMUL(GM_FADD(l.y, r.y), 0.5f);
+        l = r = make_float2(mx, my);
+    }
+}
+
 // portal k as (left, right) seen travelling from triangle k-1 to triangle k;
 // triangles that share no edge give their centroid as a point portal
 __device__ void corridor_portal(const MoverParams& p, const int* path, int start_tri, int L, float2 sp, float2 ep,
-                                int k, float2& left, float2& right) {
+                                int k, float clear, float2& left, float2& right) {
     if (k <= 0) {
         left = right = sp;
         return;
@@ -542,6 +560,7 @@ __device__ void corridor_portal(const MoverParams& p, const int* path, int start
         left = s1;
         right = s0;
     }
+    narrow_portal(left, right, clear);
 }
 
 // one thread per agent whose path starts this frame (in Move at the frame's
@@ -557,6 +576,7 @@ __global__ void k_funnel(MoverParams p) {
     float2* wp = p.waypoints + (long long)i * p.path_stride;
     const float2 sp = p.pos[i], ep = p.targ_pos[i];
     const int st = p.cur_node[i];
+    const float clear = p.sc[p.agent_scene ? p.agent_scene[i] : 0].clear;
     float2 apex = sp, fl = sp, fr = sp;
     int apex_i = 0, left_i = 0, right_i = 0, filled = 0;
     const int max_iter = 4 * (L + 2) + 16;  // every restart moves the apex forward
@@ -568,7 +588,7 @@ __global__ void k_funnel(MoverParams p) {
             break;
         }
         float2 l, r;
-        corridor_portal(p, path, st, L, sp, ep, k, l, r);
+        corridor_portal(p, path, st, L, sp, ep, k, clear, l, r);
         if (area2(apex, fr, r) >= 0.f) {  // right edge moves inward
             if (veq(apex, fr) || area2(apex, fl, r) < 0.f) {
                 fr = r;

@@ -192,7 +192,7 @@ def free_points(g: GMAPF, scn: Scenario, n: int, rng) -> np.ndarray:
 def make_world(scn: Scenario, mode: int = MODE_BATCHED, profiler: bool = False, block_threads: int = 0,
                threads_per_agent: int | None = None, queue_capacity: int | None = None, agents: int | None = None,
                parallel_agents: int | None = None, search_mem_budget: int = 0, visited_mode: int = 0,
-               autotune: bool = False, path_smoothing: bool = False, device: int = 0):
+               autotune: bool = False, path_smoothing: int = 0, device: int = 0):
     """Build a GMAPF for the scenario on CUDA device `device`; returns (g, starts, rng)."""
     A = scn.agents if agents is None else agents
     g = GMAPF()

@@ -91,9 +91,12 @@ typedef struct gmapf_options {
     int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records,
                                   3 global bitmap per slot (L2-resident for maps up to a few 100k triangles) */
     int32_t path_smoothing;    /* 1: agents steer through the corridor's funnel corners (portal edges)
-                                  instead of triangle centroids; the triangle paths and the per-triangle
-                                  progress stay the reference's.  Off (0) by default: on, agents take
-                                  different routes from the reference's (AgentsMover.h:148,174) */
+                                  instead of triangle centroids; 2: the same with every portal narrowed
+                                  by the agent radius at both ends, so the corners keep that clearance
+                                  from the walls (a portal no wider than two radii becomes its midpoint);
+                                  the triangle paths and the per-triangle progress stay the reference's.
+                                  Off (0) by default: on, agents take different routes from the
+                                  reference's (AgentsMover.h:148,174) */
     int32_t round_limit;       /* rounds one search may run before it is stopped, not found, and the
                                   call or step reports GMAPF_E_DEVICE (round-limit bit); 0 = 4 N + 64
                                   for an N-triangle map, which no search reaches (every round pops a

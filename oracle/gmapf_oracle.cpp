@@ -434,8 +434,30 @@ float orient2(float ax, float ay, float bx, float by, float cx, float cy) {
 
 /* portals 0..L+1: the start point, the shared edges (left, right as seen from
  * the earlier triangle's centroid towards the later one's), the end point */
+/* path smoothing 2: both ends of an edge portal moved inward by c (the agent
+ * radius); a portal no wider than 2c becomes its midpoint */
+void narrow_portal(float& lx, float& ly, float& rx, float& ry, float c) {
+    if (!(c > 0.0f)) return;
+    const float dx = rx - lx, dy = ry - ly;
+    const float xx = dx * dx, yy = dy * dy;
+    const float w = std::sqrt(xx + yy);
+    if (w > c + c) {
+        const float t = c / w;
+        const float ox = dx * t, oy = dy * t;
+        lx = lx + ox;
+        ly = ly + oy;
+        rx = rx - ox;
+        ry = ry - oy;
+    } else {
+        const float mx = (lx + rx) * 0.5f, my = (ly + ry) * 0.5f;
+        lx = rx = mx;
+        ly = ry = my;
+    }
+}
+
 void corridor(const Map& m, int start_tri, const std::vector<int>& path, float sx, float sy, float ex, float ey,
-              std::vector<float>& lx, std::vector<float>& ly, std::vector<float>& rx, std::vector<float>& ry) {
+              float clear, std::vector<float>& lx, std::vector<float>& ly, std::vector<float>& rx,
+              std::vector<float>& ry) {
     const int L = (int)path.size();
     lx.assign(L + 2, 0);
     ly.assign(L + 2, 0);
@@ -471,15 +493,16 @@ void corridor(const Map& m, int start_tri, const std::vector<int>& path, float s
         ly[k] = sh[2 * li + 1];
         rx[k] = sh[2 * ri];
         ry[k] = sh[2 * ri + 1];
+        narrow_portal(lx[k], ly[k], rx[k], ry[k], clear);
     }
 }
 
 /* steering point of each path step: the first funnel corner at a portal index
  * past the step's portal (step k crosses portal k + 1) */
-void funnel_points(const Map& m, Agent& ag) {
+void funnel_points(const Map& m, Agent& ag, float clear) {
     const int L = (int)ag.path.size();
     std::vector<float> lx, ly, rx, ry;
-    corridor(m, ag.cur, ag.path, ag.px, ag.py, ag.tx, ag.ty, lx, ly, rx, ry);
+    corridor(m, ag.cur, ag.path, ag.px, ag.py, ag.tx, ag.ty, clear, lx, ly, rx, ry);
     std::vector<float> cx, cy;
     std::vector<int> ci;  /* corners and their portal indices */
     float apx = ag.px, apy = ag.py, flx = apx, fly = apy, frx = apx, fry = apy;
@@ -785,7 +808,7 @@ orc_world* orc_world_create(const orc_map* m, int agents_max, float radius, floa
 }
 
 void orc_world_destroy(orc_world* w) { delete w; }
-void orc_world_set_smoothing(orc_world* w, int on) { w->smoothing = on ? 1 : 0; }
+void orc_world_set_smoothing(orc_world* w, int mode) { w->smoothing = mode == 2 ? 2 : (mode ? 1 : 0); }
 int orc_world_count(const orc_world* w) { return (int)w->a.size(); }
 
 int orc_world_add_agent(orc_world* w, float x, float y) {
@@ -859,7 +882,7 @@ void orc_world_step(orc_world* w, float dt, int threads) {
      * from the agents' positions at the frame's start */
     if (w->smoothing)
         for (int i : mv)
-            if (A[i].step_idx == -1 && !A[i].path.empty()) funnel_points(m, A[i]);
+            if (A[i].step_idx == -1 && !A[i].path.empty()) funnel_points(m, A[i], w->smoothing == 2 ? w->radius : 0.0f);
 
     /* 3. searches + path build (PathFinder.h:253-307) */
     std::vector<SearchScratch> scratch(threads);

@@ -109,8 +109,9 @@ double orc_path_len(const orc_map* m, int start, const int* path, int L);
 orc_world* orc_world_create(const orc_map* m, int agents_max, float radius, float speed,
                             int parallel_agents, int T, int C, float K);
 void orc_world_destroy(orc_world* w);
-/* path smoothing (not in the reference): steer through funnel corners */
-void orc_world_set_smoothing(orc_world* w, int on);
+/* path smoothing (not in the reference): 1 steer through funnel corners, 2 the
+ * same with every portal narrowed by the agent radius at both ends */
+void orc_world_set_smoothing(orc_world* w, int mode);
 int orc_world_add_agent(orc_world* w, float x, float y);
 int orc_world_set_target(orc_world* w, int id, float x, float y);
 void orc_world_step(orc_world* w, float dt, int threads);

@@ -237,8 +237,9 @@ class OWorld:
             self.lib.orc_world_destroy(self.h)
             self.h = None
 
-    def set_smoothing(self, on: bool):
-        self.lib.orc_world_set_smoothing(self.h, 1 if on else 0)
+    def set_smoothing(self, mode):
+        """0 / False off, 1 / True funnel corners, 2 corners one agent radius off the walls."""
+        self.lib.orc_world_set_smoothing(self.h, int(mode))
 
     def add_agent(self, x, y):
         return self.lib.orc_world_add_agent(self.h, float(x), float(y))

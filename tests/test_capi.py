@@ -96,6 +96,11 @@ def test_set_options_validates_ranges():
         g.set_options(visited_mode=vm)
     g.set_options(round_limit=500)
     assert g.options()["round_limit"] == 500
+    for sm in (0, 1, 2):
+        g.set_options(path_smoothing=sm)
+    with pytest.raises(G.GMAPFError) as e:
+        g.set_options(path_smoothing=3)
+    assert e.value.status_name == "GMAPF_E_INVALID_ARG"
 
 
 def test_fill_map_manually_checks_neighbours():

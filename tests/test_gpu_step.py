@@ -122,19 +122,33 @@ def test_zigzag_reference_driver(oracle_mod):
     run(g, ow, scn, 60, rng, check_every=20)
 
 
+@pytest.mark.parametrize("smoothing", [1, 2])
 @pytest.mark.parametrize("mode", [G.MODE_BATCHED, G.MODE_PLAIN])
-def test_path_smoothing_against_oracle(oracle_mod, mode):
+def test_path_smoothing_against_oracle(oracle_mod, mode, smoothing):
     # opt-in funnel corners instead of centroids: same triangle paths, agents
-    # steer to the corners; device and oracle funnels agree exactly
+    # steer to the corners; device and oracle funnels agree exactly.  With
+    # smoothing 2 the portals are narrowed by the agent radius at both ends.
     scn = S.cfg2()
-    g, ow, rng = make_pair(oracle_mod, scn, 512, mode=mode, smoothing=True)
+    g, ow, rng = make_pair(oracle_mod, scn, 512, mode=mode, smoothing=smoothing)
     d = run(g, ow, scn, 250, rng, retarget_every=100, check_every=25)
-    # steering points lie on corridor vertices or at the target
     tri = g.map_nodes()
-    verts = {tuple(np.float32(v)) for t in tri for v in (t["P1"], t["P2"], t["P3"])}
     moving = np.nonzero(d["state"] == G.EAgentState.Move)[0]
-    on_vertex = sum(tuple(np.float32(d["step_pos"][i])) in verts for i in moving)
-    assert len(moving) > 50 and on_vertex > 0
+    assert len(moving) > 50
+    # steering points of steps before the last (the last step steers to the target)
+    inner = moving[d["step_idx"][moving] < d["path_len"][moving]]
+    sp = np.asarray(d["step_pos"], np.float32)[inner]
+    assert len(inner) > 20
+    if smoothing == 1:
+        # steering points lie on corridor vertices or at the target
+        verts = {tuple(np.float32(v)) for t in tri for v in (t["P1"], t["P2"], t["P3"])}
+        assert sum(tuple(p) in verts for p in sp) > 0
+    else:
+        # corners keep about one radius from every vertex (a portal narrower
+        # than two radii gives its midpoint, at least as far from its ends)
+        verts = np.unique(np.concatenate([tri["P1"], tri["P2"], tri["P3"]]).astype(np.float64), axis=0)
+        dmin = np.sqrt(((sp[:, None, :].astype(np.float64) - verts[None]) ** 2).sum(-1)).min(1)
+        assert (dmin >= 0.999 * scn.radius).mean() > 0.5
+        assert (dmin > 0).all()  # none on a wall vertex
 
 
 def test_path_smoothing_shortens_routes(oracle_mod):
