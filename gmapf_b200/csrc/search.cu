@@ -670,8 +670,10 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             if (p.out_found) p.out_found[orow] = found;
             if (p.out_len) p.out_len[orow] = L;
             if (agent >= 0 && p.ag_state) {
+                // PathFinder.h:268-289: not found -> Idle with the path step
+                // index left as it was; found -> Move from step -1
                 p.ag_state[agent] = found ? GMAPF_AGENT_MOVE : GMAPF_AGENT_IDLE;
-                p.ag_step_idx[agent] = -1;
+                if (found) p.ag_step_idx[agent] = -1;
                 p.ag_path_len[agent] = L;
             }
             atomicAdd(p.stats + ST_EXPANSIONS, (unsigned long long)ex);

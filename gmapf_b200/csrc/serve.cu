@@ -101,11 +101,13 @@ __global__ void k_serve_apply(const ApplyRec* recs, int n, const int2* stash_fl,
     if (threadIdx.x == 0) {
         targ[r.agent] = r.tnode;
         targ_pos[r.agent] = make_float2(r.tx, r.ty);
-        step_idx[r.agent] = -1;
         path_len[r.agent] = ok ? L : 0;
-        // PathFinder.h:268-289: found -> Move, else Idle; an empty path means
-        // the agent already stands in the target triangle
-        state[r.agent] = (f && ok && L > 0) ? GMAPF_AGENT_MOVE : GMAPF_AGENT_IDLE;
+        // PathFinder.h:268-289: found -> Move from step -1, else Idle with the
+        // step index left as it was; an empty path means the agent already
+        // stands in the target triangle
+        const bool move = f && ok && L > 0;
+        if (move) step_idx[r.agent] = -1;
+        state[r.agent] = move ? GMAPF_AGENT_MOVE : GMAPF_AGENT_IDLE;
     }
 }
 

@@ -87,3 +87,24 @@ def test_full_frame_steps(oracle_mod):
     for i in range(0, A, 509):
         if d["path_len"][i] > 0:
             assert np.array_equal(g.path(i), ow.path(i))
+
+
+def test_full_frames_walking_with_partial_retargets(oracle_mod):
+    # 16,384 agents on the maze over 40 frames: a full retarget, then every 8
+    # frames 2,048 random agents get new targets while the others walk their
+    # long paths through each other (speed 300, so that agents cross several
+    # triangles and meet); compared with the oracle world every 4 frames
+    # (states, nodes, path steps exactly; positions within 1e-4 relative)
+    import dataclasses
+    scn = dataclasses.replace(S.cfg3(cells=160), speed=300.0)
+    A = 16384
+    g, ow, rng = make_pair(oracle_mod, scn, A, T=T, Cap=CAP, vm=3)
+    retarget(g, ow, scn, np.arange(A), rng)
+    threads = os.cpu_count() or 8
+    for block in range(5):
+        if block:
+            retarget(g, ow, scn, np.sort(rng.choice(A, 2048, replace=False)), rng)
+        d = run_steps(g, ow, scn, 8, rng, check_every=4, threads=threads)
+    moving = d["state"] == 2
+    assert moving.sum() > 0.5 * A
+    assert (d["step_idx"][moving] > 3).sum() > 0.5 * moving.sum()  # the walkers went through several triangles
