@@ -208,3 +208,24 @@ def test_collision_neighbour_counter(oracle_mod):
     st = g.last_stats()
     assert st["moving"] > 0
     assert A <= st["neighbours"] <= A * A
+
+
+@pytest.mark.parametrize("speed,mode,smoothing", [(300.0, G.MODE_BATCHED, 0), (300.0, G.MODE_PLAIN, 0),
+                                                  (60.0, G.MODE_BATCHED, 2)])
+def test_fast_crowded_walks(oracle_mod, speed, mode, smoothing):
+    # agents that cross several triangles per frame, snap onto shared
+    # centroids and collide head on (coincident agents push by 0/0 = NaN, as
+    # the reference's AgentsMover.h:108 does); a fifth retargeted every 10
+    # frames; compared with the oracle world every frame for 100 frames
+    import dataclasses
+    scn = dataclasses.replace(S.cfg2(), speed=speed)
+    A = 2048
+    g, ow, rng = make_pair(oracle_mod, scn, A, mode=mode, smoothing=smoothing)
+    retarget(g, ow, scn, np.arange(A), rng)
+    for f in range(100):
+        if f and f % 10 == 0:
+            retarget(g, ow, scn, np.sort(rng.choice(A, A // 5, replace=False)), rng)
+        g.AsyncStep(scn.dt)
+        g.WaitStepEnd()
+        ow.step(scn.dt, 8)
+        compare(g, ow, f)
