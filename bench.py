@@ -47,7 +47,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "p99 step ms & path queries/s at 16k agents, batched vs plain, on 1 B200"
 
 
-VISITED = {1: "shared-memory bitmap", 2: "query-stamped global records", 3: "global bitmap (L2-resident)"}
+VISITED = {1: "shared-memory bitmap", 2: "query-stamped global records", 3: "global bitmap (L2-resident)",
+           4: "global bitmap, moved into shared memory by a search left alone in its block"}
 
 
 def log(*a):

@@ -52,7 +52,8 @@ class Options(C.Structure):
         ("visited_mode", C.c_int32),
         ("path_smoothing", C.c_int32),
         ("round_limit", C.c_int32),
-        ("_reserved", C.c_int32 * 2),
+        ("promote_rounds", C.c_int32),
+        ("_reserved", C.c_int32 * 1),
     ]
 
 
@@ -75,7 +76,7 @@ class StepStats(C.Structure):
         ("rounds", C.c_int64), ("deg_sum", C.c_int64), ("claims", C.c_int64),
         ("path_nodes", C.c_int64), ("moving", C.c_int64),
         ("ms_step_wall", C.c_float), ("ms_search", C.c_float), ("ms_mover", C.c_float),
-        ("ms_total_device", C.c_float), ("neighbours", C.c_int64),
+        ("ms_total_device", C.c_float), ("neighbours", C.c_int64), ("promoted", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

@@ -61,11 +61,12 @@ def make_config(agents_max: int, radius: float, speed: float, parallel_agents: i
 
 def make_options(mode: int = MODE_BATCHED, device: int = 0, block_threads: int = 0, autotune: bool = False,
                  search_mem_budget: int = 0, order_by_estimate: bool = True, visited_mode: int = 0,
-                 path_smoothing: int = 0, round_limit: int = 0) -> Options:
+                 path_smoothing: int = 0, round_limit: int = 0, promote_rounds: int = 0) -> Options:
     """path_smoothing: 0 / False off, 1 / True funnel corners, 2 corners one
     agent radius off the walls."""
     o = Options()
     o.round_limit = round_limit
+    o.promote_rounds = promote_rounds
     o.path_smoothing = int(path_smoothing)
     o.device = device
     o.mode = mode
@@ -191,8 +192,8 @@ class GMAPF:
     # -- extras ------------------------------------------------------------
     def set_options(self, **kw) -> None:
         """mode, device, block_threads, autotune, search_mem_budget,
-        order_by_estimate, visited_mode, path_smoothing, round_limit (see
-        gmapf_options)."""
+        order_by_estimate, visited_mode, path_smoothing, round_limit,
+        promote_rounds (see gmapf_options)."""
         o = make_options(**kw)
         self._check(self._lib.gmapf_set_options(self._h, C.byref(o)))
 

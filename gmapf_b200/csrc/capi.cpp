@@ -198,9 +198,10 @@ gmapf_status gmapf_set_options(gmapf_ctx* ctx, const gmapf_options* o) {
         (o->block_threads < 32 || o->block_threads > 256 || o->block_threads % 32 != 0))
         return fail(GMAPF_E_INVALID_ARG, "block_threads must be 0 or a multiple of 32 in [32, 256]");
     if (o->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
-    if (o->visited_mode < 0 || o->visited_mode > 3)
-        return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
+    if (o->visited_mode < 0 || o->visited_mode > 4)
+        return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2, 3 or 4");
     if (o->round_limit < 0) return fail(GMAPF_E_INVALID_ARG, "round_limit must be >= 0 (0: no practical limit)");
+    if (o->promote_rounds < 0) return fail(GMAPF_E_INVALID_ARG, "promote_rounds must be >= 0 (0: 512)");
     if (o->path_smoothing < 0 || o->path_smoothing > 2)
         return fail(GMAPF_E_INVALID_ARG, "path_smoothing must be 0 (off), 1 (funnel corners) or 2 (corners one agent radius off the walls)");
     c.opt = *o;
@@ -315,7 +316,7 @@ uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603u
 // options the tuner reads, the GPU (name, SM count, memory) and this build,
 // so a changed map, GPU, option or library never reuses a stale shape.
 // Unreadable or foreign lines are skipped; the last matching line wins.
-const char kTuneBuild[] = "gmapf-tune 1 " __DATE__ " " __TIME__;
+const char kTuneBuild[] = "gmapf-tune 2 " __DATE__ " " __TIME__;
 
 uint64_t tune_key(const Context& c) {
     const HostMap& m = c.map;
@@ -350,7 +351,7 @@ bool tune_lookup(const std::string& path, uint64_t key, int v[4]) {
         if (std::sscanf(line, "gmapf-tune %d %16llx %d %d %d %d", &fmt, &k, &T, &C, &vm, &bt) != 6) continue;
         if (fmt != 1 || k != key) continue;
         const bool t_ok = T == 2 || T == 4 || T == 8 || T == 16 || T == 32;
-        if (!t_ok || C < 1 || vm < 0 || vm > 3 || bt < 0 || bt > 1024) continue;
+        if (!t_ok || C < 1 || vm < 0 || vm > 4 || bt < 0 || bt > 1024) continue;
         v[0] = T, v[1] = C, v[2] = vm, v[3] = bt;
         hit = true;
     }
@@ -1100,10 +1101,11 @@ gmapf_status gmapf_batch_create(gmapf_ctx* const* scenes, int32_t n, const gmapf
         if (opt->block_threads != 0 &&
             (opt->block_threads < 32 || opt->block_threads > 256 || opt->block_threads % 32 != 0))
             return fail(GMAPF_E_INVALID_ARG, "block_threads must be 0 or a multiple of 32 in [32, 256]");
-        if (opt->visited_mode < 0 || opt->visited_mode > 3)
-            return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2 or 3");
+        if (opt->visited_mode < 0 || opt->visited_mode > 4)
+            return fail(GMAPF_E_INVALID_ARG, "visited_mode must be 0 (automatic), 1, 2, 3 or 4");
         if (opt->device < 0) return fail(GMAPF_E_INVALID_ARG, "device must be >= 0");
         if (opt->round_limit < 0) return fail(GMAPF_E_INVALID_ARG, "round_limit must be >= 0");
+        if (opt->promote_rounds < 0) return fail(GMAPF_E_INVALID_ARG, "promote_rounds must be >= 0");
         if (opt->path_smoothing < 0 || opt->path_smoothing > 2)
             return fail(GMAPF_E_INVALID_ARG, "path_smoothing must be 0, 1 or 2");
     }

@@ -49,6 +49,8 @@ int search_round_limit(const Context& c) {
     return c.opt.round_limit > 0 ? c.opt.round_limit : 4 * c.map.n + 64;
 }
 
+int search_promote_rounds(const Context& c) { return c.opt.promote_rounds > 0 ? c.opt.promote_rounds : 512; }
+
 namespace {
 
 // device counters: [8] holds the frame's dt as a float
@@ -100,6 +102,7 @@ SearchParams search_params(Context& c) {
     p.gbm = d.gbm;
     p.work_ctr = d.counters + CT_WORK;
     p.max_rounds = search_round_limit(c);
+    p.promote_rounds = search_promote_rounds(c);
     p.paths = d.paths;
     p.path_stride = d.path_stride;
     p.ag_state = d.state;
@@ -232,18 +235,21 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     d.bm_words = search_bitmap_words(std::max(1, c.map.n));
 
     // Candidates: visited placement (1 shared-memory bitmap, 2 stamped
-    // records, 3 global bitmap) and block size.  The score is the number of
-    // resident slots weighted by how close the claim check is: on chip x4,
-    // L2 x3, DRAM x2 (the record check misses L2 in every round).
+    // records, 3 global bitmap, 4 global bitmap that a search left alone in
+    // its block moves into the block's shared memory) and block size.  The
+    // score is the number of resident slots weighted by how close the claim
+    // check is: on chip x4, L2 x3, DRAM x2 (the record check misses L2 in
+    // every round); placement 4 wins a tie with placement 3 (a frame's tail
+    // then checks on chip).
     long long best_score = -1;
     int best_bt = 0;
     int best_vm = 2;
     long long best_slots = 0;
     const int want_vm = c.opt.visited_mode ? c.opt.visited_mode : c.tuned_vm;
     const int want_bt = c.opt.block_threads ? c.opt.block_threads : c.tuned_bt;
-    for (int vm = 1; vm <= 3; vm++) {
+    for (int vm = 1; vm <= 4; vm++) {
         if (want_vm != 0 && want_vm != vm) continue;
-        const long long mem_slots = budget / (per_slot + (vm == 3 ? 4ll * d.bm_words : 0));
+        const long long mem_slots = budget / (per_slot + (vm >= 3 ? 4ll * d.bm_words : 0));
         const int bts[4] = {128, 64, 32, 256};
         for (int bt : bts) {
             if (want_bt != 0 && bt != want_bt) continue;
@@ -254,7 +260,7 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
             long long slots = std::min((long long)sms * per_sm * gpb, mem_slots);
             slots = (slots / gpb) * gpb;
             if (slots < gpb) continue;
-            const long long score = slots * (vm == 1 ? 4 : vm == 3 ? 3 : 2);
+            const long long score = slots * (vm == 1 ? 4 : vm >= 3 ? 3 : 2) + (vm == 4 ? 1 : 0);
             if (score > best_score) {
                 best_score = score;
                 best_bt = bt;
@@ -306,7 +312,7 @@ int alloc_search_state(Context& c, std::string& err) {
         DALLOC(d.epoch, (size_t)d.slots);
         d.rec_cap = d.slots;
     }
-    if (d.vm == 3 && (!d.gbm || d.slots > d.gbm_cap)) {
+    if (d.vm >= 3 && (!d.gbm || d.slots > d.gbm_cap)) {
         release(c, d.gbm);
         d.gbm = nullptr;
         d.gbm_cap = 0;
@@ -697,6 +703,7 @@ int device_wait_step(Context& c, std::string& err) {
     st.path_nodes = (int64_t)delta[ST_PATH_NODES];
     st.moving = (int64_t)delta[ST_MOVING];
     st.neighbours = (int64_t)delta[ST_NEIGHBOURS];
+    st.promoted = (int64_t)delta[ST_PROMOTED];
     st.ms_step_wall = std::chrono::duration<float, std::milli>(t2 - c.t_step0).count();
     st.ms_search = st.ms_mover = st.ms_total_device = 0;
     if (c.cfg.IsProfiler) {
@@ -878,6 +885,7 @@ int device_search_batch(Context& c, const int* d_starts, const int* d_targets, i
         out->deg_sum = (int64_t)(c.h_stats[ST_DEG_SUM] - before[ST_DEG_SUM]);
         out->claims = (int64_t)(c.h_stats[ST_CLAIMS] - before[ST_CLAIMS]);
         out->path_nodes = (int64_t)(c.h_stats[ST_PATH_NODES] - before[ST_PATH_NODES]);
+        out->promoted = (int64_t)(c.h_stats[ST_PROMOTED] - before[ST_PROMOTED]);
         out->ms_search = ms;
         out->ms_total_device = ms;
     }
@@ -1044,7 +1052,7 @@ int device_autotune(Context& c, std::string& err) {
     for (int T : Ts) {
         float best_at_T = 1e30f;
         for (int C : Cs)
-            for (int vm : {3, 2, 1}) {
+            for (int vm : {4, 3, 2, 1}) {
                 if (c.opt.visited_mode != 0 && c.opt.visited_mode != vm) continue;
                 const size_t before = trials.size();
                 trial(T, C, vm, 0);

@@ -41,6 +41,7 @@ enum StatIdx {
     ST_REQUESTS,
     ST_MOVING,
     ST_NEIGHBOURS,  // agents examined in the 3x3 grid cells by the collision pass
+    ST_PROMOTED,    // searches that moved their visited bitmap into their block's shared memory
     ST_COUNT
 };
 
@@ -66,6 +67,7 @@ struct SearchParams {
     unsigned* gbm;           // visited mode 3: bm_words 32-bit words per slot, global
     int* work_ctr;
     int max_rounds;
+    int promote_rounds;      // visited placement 4: rounds before a search left alone in its block moves its bitmap
     // outputs
     int* paths;              // row-major, path_stride ints per row
     long long path_stride;
@@ -179,7 +181,7 @@ void launch_prepare_batch(cudaStream_t s, const int* starts, const int* targets,
 // bitmap per slot in global memory (p.gbm, small enough to stay in L2).
 cudaError_t launch_search(cudaStream_t s, const SearchParams& p, int blocks, int block_threads,
                           bool persistent, int req_base, int vm, int bm_words);
-size_t search_smem_bytes(int C, int block_threads, int bm_words_per_group, int T);
+size_t search_smem_bytes(int C, int block_threads, int bm_words, int T, int vm);
 int search_bitmap_words(int n_nodes);
 int search_max_blocks_per_sm(int T, int C, int block_threads, int vm, int bm_words);
 
@@ -375,6 +377,7 @@ struct Context {
 // rounds one search may run: the round_limit option, else 4 N + 64 (never
 // reached: every round pops a queued node and a node is queued once)
 int search_round_limit(const Context& c);
+int search_promote_rounds(const Context& c);
 // "device-side check failed: ..." naming the ErrBits set in e
 std::string device_error_text(int e);
 int device_start(Context& c, std::string& err);

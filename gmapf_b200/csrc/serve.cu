@@ -249,6 +249,7 @@ SearchParams serve_params(Context& c, Service& sv, int k) {
     p.slot_base = k * sv.slots_per_stream;
     p.slots = sv.slots_per_stream;
     p.max_rounds = search_round_limit(c);
+    p.promote_rounds = search_promote_rounds(c);
     p.paths = sv.d_pool;
     p.path_stride = sv.stride;
     p.out_found = sv.d_found;
@@ -425,7 +426,7 @@ int serve_start(Context& c, int max_in_flight, std::string& err) {
         err = "serving: the search kernel cannot be resident with this shape";
         return GMAPF_E_CAPACITY;
     }
-    const double per_slot = (double)n * sizeof(Rec) + (d.vm == 3 ? 4.0 * d.bm_words : 0.0);
+    const double per_slot = (double)n * sizeof(Rec) + (d.vm >= 3 ? 4.0 * d.bm_words : 0.0);
     // the drain launch is persistent while queries keep coming: leave one
     // block per SM for the frames' own kernels
     const int drain_per_sm = per_sm > 1 ? per_sm - 1 : 1;
@@ -440,7 +441,7 @@ int serve_start(Context& c, int max_in_flight, std::string& err) {
     sv.slots = (int)(per_stream * kStreams);
     SALLOC(sv.rec, (size_t)sv.slots * n);
     SALLOC(sv.epoch, (size_t)sv.slots);
-    if (d.vm == 3) SALLOC(sv.gbm, (size_t)sv.slots * d.bm_words);
+    if (d.vm >= 3) SALLOC(sv.gbm, (size_t)sv.slots * d.bm_words);
     SALLOC(sv.d_stats, ST_COUNT);
 
     // ring: admission capacity from free memory (a path row and 16 bytes per entry)

@@ -192,7 +192,7 @@ def free_points(g: GMAPF, scn: Scenario, n: int, rng) -> np.ndarray:
 def make_world(scn: Scenario, mode: int = MODE_BATCHED, profiler: bool = False, block_threads: int = 0,
                threads_per_agent: int | None = None, queue_capacity: int | None = None, agents: int | None = None,
                parallel_agents: int | None = None, search_mem_budget: int = 0, visited_mode: int = 0,
-               autotune: bool = False, path_smoothing: int = 0, device: int = 0):
+               autotune: bool = False, path_smoothing: int = 0, device: int = 0, promote_rounds: int = 0):
     """Build a GMAPF for the scenario on CUDA device `device`; returns (g, starts, rng)."""
     A = scn.agents if agents is None else agents
     g = GMAPF()
@@ -200,7 +200,8 @@ def make_world(scn: Scenario, mode: int = MODE_BATCHED, profiler: bool = False, 
     g.Init(make_config(A, scn.radius, scn.speed, P, threads_per_agent or scn.threads_per_agent,
                        queue_capacity or scn.queue_capacity, scn.heuristic_k, is_profiler=profiler))
     g.set_options(mode=mode, block_threads=block_threads, search_mem_budget=search_mem_budget,
-                  visited_mode=visited_mode, autotune=autotune, path_smoothing=path_smoothing, device=device)
+                  visited_mode=visited_mode, autotune=autotune, path_smoothing=path_smoothing, device=device,
+                  promote_rounds=promote_rounds)
     build_map(g, scn)
     rng = np.random.default_rng(1000 + scn.seed)
     if scn.name == "zigzag":

@@ -89,7 +89,10 @@ typedef struct gmapf_options {
     int32_t order_by_estimate; /* 1 (default): batched form serves the searches with the largest
                                   landmark hop-distance estimate first; results do not depend on it */
     int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records,
-                                  3 global bitmap per slot (L2-resident for maps up to a few 100k triangles) */
+                                  3 global bitmap per slot (L2-resident for maps up to a few 100k triangles),
+                                  4 global bitmap per slot; a search still running after promote_rounds
+                                  rounds whose block's other warps have finished (a batch's tail) moves
+                                  its bitmap into the block's shared memory */
     int32_t path_smoothing;    /* 1: agents steer through the corridor's funnel corners (portal edges)
                                   instead of triangle centroids; 2: the same with every portal narrowed
                                   by the agent radius at both ends, so the corners keep that clearance
@@ -102,7 +105,10 @@ typedef struct gmapf_options {
                                   for an N-triangle map, which no search reaches (every round pops a
                                   queued node and a node is queued once).  Smaller values bound the
                                   time of one search */
-    int32_t _reserved[2];
+    int32_t promote_rounds;    /* visited mode 4: rounds a search runs on its global bitmap before it
+                                  may move it into its block's shared memory, 0 = 512.  Results do not
+                                  depend on it */
+    int32_t _reserved[1];
 } gmapf_options;
 
 typedef struct gmapf_step_stats {
@@ -119,6 +125,7 @@ typedef struct gmapf_step_stats {
     float ms_mover;         /* device time of the mover kernels */
     float ms_total_device;  /* device time of the whole frame */
     int64_t neighbours;     /* agents read from the 3x3 grid cells by the collision pass (summed over agents) */
+    int64_t promoted;       /* searches that moved their visited bitmap into shared memory (visited mode 4) */
 } gmapf_step_stats;
 
 typedef struct gmapf_ctx gmapf_ctx;

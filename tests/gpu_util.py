@@ -6,11 +6,18 @@ from gmapf_b200 import scenarios as S
 
 
 def map_world(scn, T=None, Cap=None, mode=G.MODE_BATCHED, agents=4, block_threads=0, visited_mode=0,
-              order=True):
+              order=True, promote_rounds=None):
+    """promote_rounds: with visited placement 4 a search moves its bitmap into
+    its block's shared memory once it has run that many rounds and the block's
+    other warps have left; by default these tests let it move from its first
+    round on."""
     g = G.GMAPF()
     g.Init(G.make_config(agents, scn.radius, scn.speed, agents, T or scn.threads_per_agent,
                          Cap or scn.queue_capacity, scn.heuristic_k))
-    g.set_options(mode=mode, block_threads=block_threads, visited_mode=visited_mode, order_by_estimate=order)
+    if promote_rounds is None:
+        promote_rounds = 1 if visited_mode == 4 else 0
+    g.set_options(mode=mode, block_threads=block_threads, visited_mode=visited_mode, order_by_estimate=order,
+                  promote_rounds=promote_rounds)
     S.build_map(g, scn)
     return g
 

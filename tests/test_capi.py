@@ -87,13 +87,15 @@ def test_bad_config_rejected():
 def test_set_options_validates_ranges():
     g = G.GMAPF()
     g.Init(G.make_config(4, 2, 1, 4, 4, 16))
-    for bad in [dict(visited_mode=4), dict(visited_mode=-1), dict(block_threads=48), dict(mode=7),
-                dict(round_limit=-1)]:
+    for bad in [dict(visited_mode=5), dict(visited_mode=-1), dict(block_threads=48), dict(block_threads=800),
+                dict(mode=7), dict(round_limit=-1), dict(promote_rounds=-1)]:
         with pytest.raises(G.GMAPFError) as e:
             g.set_options(**bad)
         assert e.value.status_name == "GMAPF_E_INVALID_ARG"
-    for vm in (0, 1, 2, 3):
+    for vm in (0, 1, 2, 3, 4):
         g.set_options(visited_mode=vm)
+    g.set_options(visited_mode=4, block_threads=128, promote_rounds=100)
+    assert g.options()["promote_rounds"] == 100
     g.set_options(round_limit=500)
     assert g.options()["round_limit"] == 500
     for sm in (0, 1, 2):

@@ -1,7 +1,9 @@
 """The bench frame's size and shape: the ~100k-triangle maze (160x160 cells,
 101,698 triangles), 16,384 searches in one batch, 32 threads per agent and
 queue capacity 16 (the shape the autotuner picks for this map), visited
-bitmap in global memory.  Checked through properties that do not depend on
+bitmap in global memory (placement 3) or in global memory and then, for a
+search left alone in its block, in shared memory (placement 4, the default
+pick).  Checked through properties that do not depend on
 size: two runs agree bit for bit, a sample agrees with the oracle exactly,
 paths are connected chains of neighbours that end at their targets, and no
 path is shorter than the BFS optimum.  The per-frame step at the same size
@@ -33,15 +35,19 @@ def run(g, s, t):
     return f, ln, p, st
 
 
-def test_full_frame_batch(oracle_mod):
+@pytest.mark.parametrize("vm", [3, 4])
+def test_full_frame_batch(oracle_mod, vm):
+    # placement 4 at its default: searches alone in their blocks move after 512 rounds
     scn = S.cfg3(cells=160)
-    g = map_world(scn, T=T, Cap=CAP, visited_mode=3)
+    g = map_world(scn, T=T, Cap=CAP, visited_mode=vm, promote_rounds=0)
     assert g.node_count > 100_000
     s, t = random_queries(g, scn, N_QUERIES, seed=31)
     f1, l1, p1, st1 = run(g, s, t)
     f2, l2, p2, st2 = run(g, s, t)
     assert torch.equal(f1, f2) and torch.equal(l1, l2) and torch.equal(p1, p2)
     assert st1["rounds"] == st2["rounds"] and st1["expansions"] == st2["expansions"]
+    if vm == 4:
+        assert st1["promoted"] > 0 and st2["promoted"] > 0  # the long searches moved
     f, ln = f1.cpu().numpy(), l1.cpu().numpy()
     assert f.sum() >= 0.99 * N_QUERIES  # the maze is connected; losses come only from bounded queues
 
@@ -73,14 +79,15 @@ def test_full_frame_batch(oracle_mod):
     assert np.all(ln[idx] >= hops)
 
 
-def test_full_frame_steps(oracle_mod):
+@pytest.mark.parametrize("vm", [3, 4])
+def test_full_frame_steps(oracle_mod, vm):
     # the step itself at this size: 16,384 agents all retargeted in one frame
     # (compaction, search, path rows), then two frames of movement and
     # collisions, each compared with the oracle world (states, nodes, path
     # steps exactly; positions within 1e-4 relative)
     scn = S.cfg3(cells=160)
     A = 16384
-    g, ow, rng = make_pair(oracle_mod, scn, A, T=T, Cap=CAP, vm=3)
+    g, ow, rng = make_pair(oracle_mod, scn, A, T=T, Cap=CAP, vm=vm, promote_rounds=0)
     retarget(g, ow, scn, np.arange(A), rng)
     d = run_steps(g, ow, scn, 3, rng, check_every=1, threads=os.cpu_count() or 8)
     assert (d["path_len"] > 0).sum() >= 0.99 * A

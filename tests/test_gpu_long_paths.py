@@ -49,12 +49,12 @@ def queries():
 
 
 @pytest.mark.parametrize("T,Cap", [(32, 16), (16, 16), (8, 32)])
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 def test_long_corridor_paths(oracle_mod, T, Cap, vm):
     nodes = corridor(N)
     g = G.GMAPF()
     g.Init(G.make_config(4, 0.1, 1.0, 4, T, Cap))
-    g.set_options(visited_mode=vm)
+    g.set_options(visited_mode=vm, promote_rounds=300 if vm == 4 else 0)  # 4: searches move after 300 rounds
     g.FillMapManually(nodes)
     g.ManualStart()
     s, t = queries()

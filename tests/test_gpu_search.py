@@ -28,7 +28,7 @@ def check_batch(oracle_mod, g, starts, targets, T, Cap, K=1.0):
     return f, l, p, st
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 @pytest.mark.parametrize("T,Cap", [(2, 1), (2, 16), (4, 16), (8, 2), (32, 64)])
 def test_cfg1_all_pairs(oracle_mod, T, Cap, vm):
     scn = S.cfg1()
@@ -39,7 +39,7 @@ def test_cfg1_all_pairs(oracle_mod, T, Cap, vm):
     assert f.mean() > 0.5
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 @pytest.mark.parametrize("T,Cap", [(8, 32), (4, 16), (16, 8)])
 def test_cfg2_random(oracle_mod, T, Cap, vm):
     scn = S.cfg2()
@@ -48,7 +48,7 @@ def test_cfg2_random(oracle_mod, T, Cap, vm):
     check_batch(oracle_mod, g, s, t, T, Cap)
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 @pytest.mark.parametrize("T,Cap", [(8, 32), (32, 64), (2, 256), (16, 16)])
 def test_maze64_random(oracle_mod, T, Cap, vm):
     scn = S.cfg3(cells=64)
@@ -65,7 +65,23 @@ def test_maze64_random(oracle_mod, T, Cap, vm):
                 assert b in nb[a]
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("T,Cap", [(32, 16), (8, 32), (4, 16)])
+def test_alone_search_moves_to_shared_memory(oracle_mod, T, Cap):
+    # visited placement 4: a search still running once the other warps of its
+    # block have left moves its queues and visited bitmap into the block's
+    # shared memory and finishes there; batches of three queries leave most
+    # searches alone in their blocks, so both kinds of rounds and the move
+    # between them are compared with the oracle
+    scn = S.cfg3(cells=64)
+    g = map_world(scn, T=T, Cap=Cap, visited_mode=4, promote_rounds=1)
+    s, t = random_queries(g, scn, 24, seed=41)
+    moved = 0
+    for k in range(0, 24, 3):
+        moved += check_batch(oracle_mod, g, s[k:k + 3], t[k:k + 3], T, Cap)[3]["promoted"]
+    assert moved > 0
+
+
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 def test_plain_equals_batched(oracle_mod, vm):
     scn = S.cfg2()
     gb = map_world(scn, T=8, Cap=32, mode=G.MODE_BATCHED, visited_mode=vm)
@@ -85,7 +101,7 @@ def test_autotune_picks_a_shape_and_stays_exact(oracle_mod):
     g.ManualStart()
     sh = g.search_shape()
     assert sh["T"] in (2, 4, 8, 16, 32) and sh["C"] in (8, 16, 32, 64, 128, 256)
-    assert sh["visited_mode"] in (1, 2, 3) and sh["block_threads"] in (32, 64, 128, 256)
+    assert sh["visited_mode"] in (1, 2, 3, 4) and sh["block_threads"] in (32, 64, 128, 256, 384, 512, 768)
     s, t = random_queries(g, scn, 1000, seed=17)
     check_batch(oracle_mod, g, s, t, sh["T"], sh["C"])
 
@@ -195,7 +211,7 @@ def test_block_shape_does_not_change_results(oracle_mod, bt):
     check_batch(oracle_mod, g, s, t, 4, 16)
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 def test_edge_cases(oracle_mod, vm):
     scn = S.cfg1()
     g = map_world(scn, T=4, Cap=16, visited_mode=vm)
@@ -218,12 +234,12 @@ def test_edge_cases(oracle_mod, vm):
     assert all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 def test_disconnected_map_not_found(oracle_mod, vm):
     # two separate triangles: searches between them exhaust both queues
     g = G.GMAPF()
     g.Init(G.make_config(4, 1, 1, 4, 4, 16))
-    g.set_options(visited_mode=vm)
+    g.set_options(visited_mode=vm, promote_rounds=1 if vm == 4 else 0)
     nodes = np.zeros(4, G.NODE_DTYPE)
     nodes["P1"] = [[0, 0], [1, 0], [10, 0], [11, 0]]
     nodes["P2"] = [[1, 0], [1, 1], [11, 0], [11, 1]]

@@ -10,9 +10,15 @@ from gpu_util import close_rel
 pytestmark = pytest.mark.gpu
 
 
-def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None, vm=0, smoothing=False):
+def make_pair(oracle_mod, scn, agents, mode=G.MODE_BATCHED, T=None, Cap=None, P=None, vm=0, smoothing=False,
+              promote_rounds=None):
+    # visited placement 4: by default a search may move its bitmap into its
+    # block's shared memory from its first round on
+    if promote_rounds is None:
+        promote_rounds = 1 if vm == 4 else 0
     g, starts, rng = S.make_world(scn, mode=mode, agents=agents, threads_per_agent=T, queue_capacity=Cap,
-                                  parallel_agents=P, visited_mode=vm, path_smoothing=smoothing)
+                                  parallel_agents=P, visited_mode=vm, path_smoothing=smoothing,
+                                  promote_rounds=promote_rounds)
     om = oracle_mod.OMap(g.map_nodes())
     ow = oracle_mod.OWorld(om, agents, scn.radius, scn.speed, P or agents, T or scn.threads_per_agent,
                            Cap or scn.queue_capacity, scn.heuristic_k)
@@ -69,7 +75,7 @@ def test_cfg1_200_steps(oracle_mod):
     assert np.array_equal(pos, d["pos"], equal_nan=True)
 
 
-@pytest.mark.parametrize("vm", [1, 2, 3])
+@pytest.mark.parametrize("vm", [1, 2, 3, 4])
 def test_cfg2_retargets(oracle_mod, vm):
     scn = S.cfg2()
     g, ow, rng = make_pair(oracle_mod, scn, 512, vm=vm)
