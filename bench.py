@@ -991,8 +991,9 @@ def profile_search(spec: str, budget_mb: int, timeline: bool):
     the batched-uneven-queries configuration, draws QUERIES seeded free-space
     start/target pairs (numpy default_rng(7), starts then targets) and runs
     gmapf_search_batch_host once with threads per agent T, queue capacity C
-    and visited mode 1 (shared-memory bitmap), 2 (global records) or 3
-    (global bitmap); budget_mb caps the search state (and so the resident
+    and visited mode 1 (shared-memory bitmap), 2 (global records), 3
+    (global bitmap) or 4 (global bitmap, moved into shared memory by a search
+    left alone in its block); budget_mb caps the search state (and so the resident
     slots) to keep a capture small.  Paths are not kept (2-entry rows: long
     paths raise the path-capacity flag, which is expected).  With timeline,
     each request's start and end on the GPU global timer are recorded
@@ -1016,7 +1017,7 @@ def profile_search(spec: str, budget_mb: int, timeline: bool):
     st = g.search_batch(s, t, 2, check=False)[3]  # long paths overflow the 2-entry rows: expected
     out = {"search_ms": g.last_search_ms(), "shape": g.search_shape()}
     out["stats"] = {k: st[k] for k in ("requests", "found", "rounds", "expansions", "claims", "deg_sum",
-                                       "path_nodes")}
+                                       "path_nodes", "promoted")}
     if timeline:
         out["timeline"] = timeline_summary(buf.cpu().numpy().reshape(nq, 2), g.search_shape()["slots"])
     print(json.dumps(out), flush=True)

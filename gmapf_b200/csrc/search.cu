@@ -410,11 +410,12 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
 
         unsigned expansions = 0, deg_sum = 0, claims = 2, rounds = 0;
         int found = 0, mS = -1, gS = 0, mT = -1, gT = 0;
+        int next_check = p.promote_rounds;  // placement 4: the round of the next alone-in-block check
 
         // ------------------------------------------------------------ rounds
         // The rounds with the claim checks in placement VX (1 shared, 2
         // records, 3 global bitmap) on bitmap bmx.  Returns true when the
-        // search leaves to continue in its block's region (placement 4).
+        // search leaves to continue in its block's shared memory (placement 4).
         auto run_rounds = [&](auto vtag, unsigned* bmx) -> bool {
           constexpr int VX = decltype(vtag)::value;
           constexpr bool SMX = VX == 1;
@@ -679,8 +680,9 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
             __syncwarp();  // frontier reads done before the next round rewrites it
             if (ended) return false;
             if constexpr (VM == 4 && VX == 3) {
-                // from promote_rounds on, every 256 rounds: alone in the block?
-                if ((int)rounds >= p.promote_rounds && (((int)rounds - p.promote_rounds) & 255) == 0) {  // warp-uniform
+                // at promote_rounds rounds, then every 256: alone in the block?
+                if ((int)rounds == next_check) {  // warp-uniform
+                    next_check += 256;
                     int alone = 0;
                     if (lane == 0) alone = *reinterpret_cast<volatile int*>(&block_active) == 1;
                     if (__shfl_sync(kFull, alone, 0)) return true;
