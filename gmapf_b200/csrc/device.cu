@@ -1051,17 +1051,26 @@ int device_autotune(Context& c, std::string& err) {
     long long best_found_so_far = 0;
     for (int T : Ts) {
         float best_at_T = 1e30f;
-        for (int C : Cs)
+        for (int C : Cs) {
+            bool vm4_fits = false;
             for (int vm : {4, 3, 2, 1}) {
                 if (c.opt.visited_mode != 0 && c.opt.visited_mode != vm) continue;
+                // placement 4 runs placement 3's rounds until a search is alone in
+                // its block, then cheaper ones: where it fits with placement 3's
+                // occupancy, 3 is not timed
+                if (vm == 3 && vm4_fits) continue;
                 const size_t before = trials.size();
                 trial(T, C, vm, 0);
                 if (trials.size() == before) continue;  // shape does not fit this placement
+                if (vm == 4)
+                    vm4_fits = search_max_blocks_per_sm(T, C, c.block_threads, 4, d.bm_words) ==
+                               search_max_blocks_per_sm(T, C, c.block_threads, 3, d.bm_words);
                 best_at_T = std::min(best_at_T, trials.back().ms);
                 const long long f = trials.back().found;
                 best_found_so_far = std::max(best_found_so_far, f);
                 if ((double)f < (double)best_found_so_far * 0.999) break;
             }
+        }
         if (best_at_T < 1e30f && best_at_T > 2.0f * best_so_far) break;
     }
     auto choose = [&]() -> const Trial* {
