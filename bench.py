@@ -838,7 +838,8 @@ def bench_b200(args):
         g2.close()
 
     if rank == 0:
-        st_sum = {k: sum(s[k] for s in dstats) for k in ["requests", "found", "expansions", "rounds", "claims"]}
+        st_sum = {k: sum(s[k] for s in dstats) for k in ["requests", "found", "expansions", "rounds", "claims",
+                                                          "promoted"]}
         clocks = clk.summary()
         cfg = workload_config(args, n_nodes, A, shape["T"], shape["C"])
         cfg.update({"l2": "flushed between frames (256 MB write); per-frame search records exceed L2",
@@ -861,7 +862,10 @@ def bench_b200(args):
                       "autotuner_pick": {"threads_per_agent": pick[0], "queue_capacity": pick[1]},
                       "start_s": round(g.startup_s, 2), "config_threads_per_agent": Tc,
                       "config_queue_capacity": Cc, "visited_mode": VISITED[shape["visited_mode"]],
-                      "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)"},
+                      "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",
+                      # visited placement 4: searches per frame that were left alone in their
+                      # block and moved their visited bitmap into shared memory
+                      "moved_to_shared_per_frame": st_sum["promoted"] / max(1, K)},
             "p99_step_ms": pct(parts["step"], 99),
             "p50_step_ms": pct(parts["step"], 50),
             "device_ms_per_step": {"mean": statistics.mean(ms), "p50": pct(ms, 50), "p99": pct(ms, 99),
