@@ -75,11 +75,12 @@ def run(scns, scenes, worlds, rngs, batch, steps, p_retarget=0.02, check_every=2
                 compare(g, ow, f"scene {s}, step {k}")
 
 
-@pytest.mark.parametrize("vm", [0, 3])
+@pytest.mark.parametrize("vm", [0, 3, 4])
 def test_batch_matches_scenes_alone(oracle_mod, vm):
+    # visited placement 4: searches may move into shared memory from their first round on
     scns = S.cfg4(6, seed=9, agents_range=(40, 160))
     scenes, worlds, rngs = build(oracle_mod, scns)
-    batch = G.SceneBatch(scenes, visited_mode=vm)
+    batch = G.SceneBatch(scenes, visited_mode=vm, promote_rounds=1 if vm == 4 else 0)
     run(scns, scenes, worlds, rngs, batch, 80)
     # paths, in each scene's own triangle ids
     for g, ow in zip(scenes, worlds):

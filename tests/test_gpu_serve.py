@@ -12,7 +12,9 @@ pytestmark = pytest.mark.gpu
 
 
 def world(scn, agents, T=8, Cap=32, vm=0):
-    g, starts, rng = S.make_world(scn, agents=agents, threads_per_agent=T, queue_capacity=Cap, visited_mode=vm)
+    # visited placement 4: searches may move into shared memory from their first round on
+    g, starts, rng = S.make_world(scn, agents=agents, threads_per_agent=T, queue_capacity=Cap, visited_mode=vm,
+                                  promote_rounds=1 if vm == 4 else 0)
     g.ManualStart()
     return g, starts, rng
 
@@ -27,7 +29,7 @@ def oracle_check(oracle_mod, g, T, Cap, starts, targets, results):
             assert np.array_equal(rp, p[i, :l[i]]), f"query {i}: path differs"
 
 
-@pytest.mark.parametrize("vm", [1, 3])
+@pytest.mark.parametrize("vm", [1, 3, 4])
 def test_serve_matches_oracle_and_installs_paths(oracle_mod, vm):
     scn = S.cfg2()
     g, starts, rng = world(scn, 600, vm=vm)
