@@ -117,3 +117,9 @@ def test_search_side_counters(bench):
     d = bench.search_side_counters(32, 16, 3, rounds=35_000_000, search_ms=30.0)
     assert 100 < d["l2_gbs"] < 20000 and 0 < d["threads_per_warp_instruction"] <= 32
     assert bench.search_side_counters(2, 8, 1, 1, 1.0) == {}
+
+
+def test_every_visited_placement_has_a_name(bench):
+    # the bench line names the visited placement the library picked; every
+    # placement gmapf_options.visited_mode accepts (1..4) has a name
+    assert set(bench.VISITED) == {1, 2, 3, 4}

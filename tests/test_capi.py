@@ -35,6 +35,38 @@ def test_config_layout_matches_reference():
     assert Node.NeibsIdx.offset == 32
 
 
+def test_ctypes_mirrors_match_the_c_header(tmp_path):
+    # every struct the Python binding passes through the C ABI has the C
+    # header's size and field offsets (a C program built against
+    # include/gmapf_c.h prints them)
+    import ctypes as C
+    import shutil
+    import subprocess
+    from gmapf_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"gmapf_config": _lib.Config, "gmapf_v2": _lib.V2, "gmapf_node": _lib.Node,
+               "gmapf_options": _lib.Options, "gmapf_step_stats": _lib.StepStats,
+               "gmapf_serve_stats": _lib.ServeStats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "gmapf_c.h"', "int main(void) {"]
+    for name, cls in mirrors.items():
+        lines.append(f'printf("{name} sizeof %zu\\n", sizeof({name}));')
+        for f, _ in cls._fields_:
+            lines.append(f'printf("{name} {f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", str(HDR.parent), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for name, cls in mirrors.items():
+        assert got[(name, "sizeof")] == C.sizeof(cls), name
+        for f, _ in cls._fields_:
+            assert got[(name, f)] == getattr(cls, f).offset, (name, f)
+
+
 def test_lifecycle_rules():
     g = G.GMAPF()
     with pytest.raises(G.GMAPFError) as e:
