@@ -92,7 +92,10 @@ typedef struct gmapf_options {
                                   3 global bitmap per slot (L2-resident for maps up to a few 100k triangles),
                                   4 global bitmap per slot; a search still running after promote_rounds
                                   rounds whose block's other warps have finished (a batch's tail) moves
-                                  its bitmap into the block's shared memory */
+                                  its bitmap into the block's shared memory (the bitmap, N/4 bytes for
+                                  N triangles, has to fit in one block's shared memory; automatic
+                                  placement only picks 4 where it does, a forced 4 that does not fit
+                                  fails the start with GMAPF_E_CAPACITY) */
     int32_t path_smoothing;    /* 1: agents steer through the corridor's funnel corners (portal edges)
                                   instead of triangle centroids; 2: the same with every portal narrowed
                                   by the agent radius at both ends, so the corners keep that clearance
