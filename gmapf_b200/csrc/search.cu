@@ -34,8 +34,8 @@
 //   - visited state, one of four placements: a 2-bit-per-node bitmap
 //     (claimed, side) per slot in shared memory; the same bitmap per slot in
 //     global memory, sized to stay in L2 and cleared per query; that global
-//     bitmap, moved into the block's shared memory by a search still running
-//     once the rest of its block has finished (a batch's tail); or the
+//     bitmap, moved into the shares of its block's finished warps by a search
+//     still running at a batch's tail; or the
 //     32-byte records themselves, stamped with the query epoch (no clearing
 //     between queries, but one DRAM round trip per round);
 //   - for T >= 16 the expanded node's parent (carried in its frontier entry)
@@ -171,9 +171,44 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
 }
 
 
+// Placement 4: words after the last warp's share so that all but one share
+// and the pad hold one bitmap (a multiple of 4 words).
+__host__ __device__ __forceinline__ size_t search_pad_words(int bm_words, int warps, int per_warp) {
+    const long long rest = (long long)bm_words - (long long)(warps - 1) * per_warp;
+    return rest > 0 ? (size_t)((rest + 3) & ~3ll) : 0;
+}
+
 // Record word 0 in the bitmap placements: the nearest proper ancestor whose
 // depth (G) is a multiple of kJumpDepth, -1 at a search's root.
 constexpr int kJumpDepth = 256;
+
+// Placement 4: where a search of warp `me` can put its bitmap (bm words) in
+// its block's shared memory, given the warps that have left (`left`, whose
+// shares are free for good).  Shares are `share` words each, `pad` words
+// follow the last one.  The bitmap takes a run of free shares (this warp's
+// own share may be in it), the last run of the block also using the pad;
+// when this warp's share is in the run, its queues move to a free share
+// outside it.  Returns first | home << 8, or -1 when there is no room.
+__device__ __noinline__ int region_plan(unsigned left, int me, int wpb, int share, int bm, int pad) {
+    if (pad >= bm) return wpb | (me << 8);  // the pad alone (one-warp blocks)
+    const unsigned usable = left | (1u << me);
+    for (int first = wpb - 1; first >= 0; first--) {
+        // the run [first, last] with the smallest last that holds the bitmap
+        long long room = 0;
+        int last = first;
+        for (; last < wpb; last++) {
+            if (!((usable >> last) & 1u)) break;
+            room += share + (last == wpb - 1 ? pad : 0);
+            if (room >= bm) break;
+        }
+        if (last >= wpb || room < bm || !((usable >> last) & 1u)) continue;
+        const unsigned run = (last - first >= 31 ? 0xffffffffu : ((2u << (last - first)) - 1u)) << first;
+        if (!((run >> me) & 1u)) return first | (me << 8);
+        const unsigned outside = left & ~run;  // another free share for this warp's queues
+        if (outside) return first | ((__ffs(outside) - 1) << 8);
+    }
+    return -1;
+}
 
 // Path output: depth d of the start side at out[d - 1] (d >= 1), depth d of
 // the target side at out[gS + gT - d] (d >= 0).
@@ -274,17 +309,19 @@ __device__ __forceinline__ void walk_path(const Rec* rec, int n_nodes, int* out,
 // among its threads).
 //
 // Placement 4: the block's shared memory holds each warp's queues and
-// frontier contiguously, plus a pad sized so that everything after the first
-// warp's share can hold one visited bitmap.  A search runs on its slot's
-// global bitmap (placement 3's rounds); from p.promote_rounds rounds on, every
-// 256 rounds, it checks whether it is the last warp of its block still
-// running (the others have left the persistent loop: the work queue is empty).
-// If so it moves its queues and frontier into the first warp's share, copies
-// its bitmap into the rest and runs its remaining rounds with the claim checks
-// in shared memory (placement 1's rounds).  Alone, a round with the check in
-// shared memory is ~15-18% shorter on the 101,698-triangle maze, and a frame's
-// tail is its longest searches running alone in their blocks.  Results do not
-// depend on where the bitmap is.
+// frontier contiguously, plus a pad sized so that all shares but one, with
+// the pad, can hold one visited bitmap.  A search runs on its slot's global
+// bitmap (placement 3's rounds); from p.promote_rounds rounds on, every 256
+// rounds, it checks whether enough warps of its block have left the
+// persistent loop (the work queue is empty: they never come back) for a run
+// of their shares to hold its bitmap.  If so, and no other search of the
+// block is in shared memory, it copies its bitmap into that run (its queues
+// and frontier move to another free share when its own lies in the run) and
+// runs its remaining rounds with the claim checks in shared memory
+// (placement 1's rounds), then returns to its own share.  Alone, a round with
+// the check in shared memory is ~15-18% shorter on the 101,698-triangle maze,
+// and a frame's tail is its longest searches running on a nearly idle GPU.
+// Results do not depend on where the bitmap is.
 template <int T, int VM>
 __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persistent, int req_base, int bm_words) {
     constexpr bool SMEMV = VM == 1;  // bitmap in shared memory
@@ -298,9 +335,17 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
     const int n_nodes = p.n;
     const float K = p.K;
     const int C = p.C;
-    __shared__ int block_active;  // placement 4: warps of this block still in the persistent loop
+    // placement 4: the warps of this block that have left the persistent loop
+    // (or never entered it; their shares stay free) and the warp whose search
+    // runs in the block's shared memory (-1: none)
+    __shared__ unsigned block_left;
+    __shared__ int block_mover;
     if constexpr (VM == 4) {
-        if (threadIdx.x == 0) block_active = max(0, min(wpb, p.slots - (int)blockIdx.x * wpb));
+        if (threadIdx.x == 0) {
+            const int valid = max(0, min(wpb, p.slots - (int)blockIdx.x * wpb));
+            block_left = (wpb >= 32 ? 0xffffffffu : ((1u << wpb) - 1u)) & ~((valid >= 32 ? 0xffffffffu : (1u << valid) - 1u));
+            block_mover = -1;
+        }
         __syncthreads();
     }
 
@@ -410,12 +455,13 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
 
         unsigned expansions = 0, deg_sum = 0, claims = 2, rounds = 0;
         int found = 0, mS = -1, gS = 0, mT = -1, gT = 0;
-        int next_check = p.promote_rounds;  // placement 4: the round of the next alone-in-block check
+        int next_check = p.promote_rounds;  // placement 4: the round of the next room-in-block check
 
         // ------------------------------------------------------------ rounds
         // The rounds with the claim checks in placement VX (1 shared, 2
         // records, 3 global bitmap) on bitmap bmx.  Returns true when the
-        // search leaves to continue in its block's shared memory (placement 4).
+        // search has ended, false when (placement 4) enough warps of its block
+        // have left for its bitmap to fit in their shares.
         auto run_rounds = [&](auto vtag, unsigned* bmx) -> bool {
           constexpr int VX = decltype(vtag)::value;
           constexpr bool SMX = VX == 1;
@@ -678,41 +724,67 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 }
             }
             __syncwarp();  // frontier reads done before the next round rewrites it
-            if (ended) return false;
+            if (ended) return true;
             if constexpr (VM == 4 && VX == 3) {
-                // at promote_rounds rounds, then every 256: alone in the block?
+                // at promote_rounds rounds, then every 256: enough shares free
+                // (their count; where the bitmap goes is worked out outside)?
                 if ((int)rounds == next_check) {  // warp-uniform
                     next_check += 256;
-                    int alone = 0;
-                    if (lane == 0) alone = *reinterpret_cast<volatile int*>(&block_active) == 1;
-                    if (__shfl_sync(kFull, alone, 0)) return true;
+                    int room = 0;
+                    if (lane == 0) {
+                        const int share = (int)(qblk + fblk);
+                        const int rest = bm_words - (int)search_pad_words(bm_words, wpb, share);
+                        const int need = rest > 0 ? (rest + share - 1) / share : 0;
+                        room = __popc(*reinterpret_cast<volatile unsigned*>(&block_left) | (1u << wib)) >= need;
+                    }
+                    if (__shfl_sync(kFull, room, 0)) return false;
                 }
             }
           }
         };
         if constexpr (VM == 4) {
-            if (run_rounds(std::integral_constant<int, 3>{}, bm)) {
-                // the block's other warps have left: move this warp's queues and
-                // frontier into the first share (the deferred items stay in place
-                // in the frontier), then the bitmap into the rest of the block's
-                // shared memory, and go on there
+            int move_plan = -1;
+            while (!run_rounds(std::integral_constant<int, 3>{}, bm)) {
+                if (lane == 0) {
+                    move_plan = region_plan(*reinterpret_cast<volatile unsigned*>(&block_left), wib, wpb,
+                                            (int)(qblk + fblk), bm_words,
+                                            (int)search_pad_words(bm_words, wpb, (int)(qblk + fblk)));
+                    if (move_plan >= 0 && atomicCAS(&block_mover, -1, wib) != -1) move_plan = -1;
+                }
+                move_plan = __shfl_sync(kFull, move_plan, 0);
+                if (move_plan >= 0) break;  // else back to the rounds: the next check in 256
+            }
+            if (move_plan >= 0) {
+                // shares of warps that have left hold the bitmap from share
+                // `first` on; this warp's queues and frontier move to share `home`
+                // when its own share lies in that run (the deferred items stay in
+                // place in the frontier); the search goes on there
                 __threadfence_block();
-                int* home = base;
-                if (ring.base != home) {
+                const int first = move_plan & 0xff, home = move_plan >> 8;
+                if (home != wib) {
                     const int4* from = reinterpret_cast<const int4*>(ring.base);
-                    int4* to = reinterpret_cast<int4*>(home);
+                    int4* to = reinterpret_cast<int4*>(base + (size_t)home * (qblk + fblk));
                     for (int k = lane; k < (int)((qblk + fblk) >> 2); k += 32) to[k] = from[k];
                     __syncwarp();
-                    ring.base = home;
-                    fr = home + qblk;
+                    ring.base = base + (size_t)home * (qblk + fblk);
+                    fr = ring.base + qblk;
                 }
-                unsigned* region = reinterpret_cast<unsigned*>(home + qblk + fblk);
+                unsigned* region = reinterpret_cast<unsigned*>(base + (size_t)first * (qblk + fblk));
                 const uint4* g4 = reinterpret_cast<const uint4*>(bm);
                 uint4* s4 = reinterpret_cast<uint4*>(region);
                 for (int k = lane; k < (bm_words >> 2); k += 32) s4[k] = __ldcg(g4 + k);
                 __syncwarp();
                 run_rounds(std::integral_constant<int, 1>{}, region);
-                if (lane == 0) atomicAdd(p.stats + ST_PROMOTED, 1ull);
+                // back to the warp's own share (the next query starts afresh) and
+                // the block's shared memory free for another search
+                ring.base = base + (size_t)wib * (qblk + fblk);
+                fr = ring.base + qblk;
+                __syncwarp();
+                __threadfence_block();
+                if (lane == 0) {
+                    atomicExch(&block_mover, -1);
+                    atomicAdd(p.stats + ST_PROMOTED, 1ull);
+                }
             }
         } else {
             run_rounds(std::integral_constant<int, VM>{}, bm);
@@ -756,7 +828,7 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
     if constexpr (VM == 4) {  // this warp uses its block's shared memory no more
         __syncwarp();
         __threadfence_block();
-        if (lane == 0) atomicSub(&block_active, 1);
+        if (lane == 0) atomicOr(&block_left, 1u << wib);
     }
 }
 
@@ -847,8 +919,7 @@ int occupancy_v(int T, int C, int bt, int bm_words) {
 size_t search_smem_bytes(int C, int bt, int bm_words, int T, int vm) {
     const size_t warps = (size_t)bt / 32;
     const size_t per_warp = search_queue_words(C, T) + search_frontier_words(T);
-    size_t pad = 0;
-    if (vm == 4 && (size_t)bm_words > (warps - 1) * per_warp) pad = (((size_t)bm_words - (warps - 1) * per_warp) + 3) & ~(size_t)3;
+    const size_t pad = vm == 4 ? search_pad_words(bm_words, (int)warps, (int)per_warp) : 0;
     return 4 * (warps * (per_warp + (vm == 1 ? (size_t)bm_words : 0)) + pad);
 }
 

@@ -91,8 +91,8 @@ typedef struct gmapf_options {
     int32_t visited_mode;      /* 0 automatic, 1 shared-memory bitmap per slot, 2 stamped global records,
                                   3 global bitmap per slot (L2-resident for maps up to a few 100k triangles),
                                   4 global bitmap per slot; a search still running after promote_rounds
-                                  rounds whose block's other warps have finished (a batch's tail) moves
-                                  its bitmap into the block's shared memory (the bitmap, N/4 bytes for
+                                  rounds, once enough of its block's warps have finished (a batch's
+                                  tail), moves its bitmap into their shared memory (the bitmap, N/4 bytes for
                                   N triangles, has to fit in one block's shared memory; automatic
                                   placement only picks 4 where it does, a forced 4 that does not fit
                                   fails the start with GMAPF_E_CAPACITY) */
