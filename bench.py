@@ -48,7 +48,7 @@ METRIC = "p99 step ms & path queries/s at 16k agents, batched vs plain, on 1 B20
 
 
 VISITED = {1: "shared-memory bitmap", 2: "query-stamped global records", 3: "global bitmap (L2-resident)",
-           4: "global bitmap, moved into shared memory by a search left alone in its block"}
+           4: "global bitmap, moved into shared memory by a search still running at the batch's tail"}
 
 
 def log(*a):
@@ -863,8 +863,8 @@ def bench_b200(args):
                       "start_s": round(g.startup_s, 2), "config_threads_per_agent": Tc,
                       "config_queue_capacity": Cc, "visited_mode": VISITED[shape["visited_mode"]],
                       "slots": shape["slots"], "form": "batched (persistent search, CUDA graph)",
-                      # visited placement 4: searches per frame that were left alone in their
-                      # block and moved their visited bitmap into shared memory
+                      # visited placement 4: searches per frame that moved their visited
+                      # bitmap into the shared memory of their block's finished warps
                       "moved_to_shared_per_frame": st_sum["promoted"] / max(1, K)},
             "p99_step_ms": pct(parts["step"], 99),
             "p50_step_ms": pct(parts["step"], 50),
@@ -997,7 +997,7 @@ def profile_search(spec: str, budget_mb: int, timeline: bool):
     gmapf_search_batch_host once with threads per agent T, queue capacity C
     and visited mode 1 (shared-memory bitmap), 2 (global records), 3
     (global bitmap) or 4 (global bitmap, moved into shared memory by a search
-    left alone in its block); budget_mb caps the search state (and so the resident
+    still running at the batch's tail); budget_mb caps the search state (and so the resident
     slots) to keep a capture small.  Paths are not kept (2-entry rows: long
     paths raise the path-capacity flag, which is expected).  With timeline,
     each request's start and end on the GPU global timer are recorded

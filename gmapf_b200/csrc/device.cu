@@ -235,8 +235,8 @@ int pick_slots(Context& c, int& blocks, std::string& err) {
     d.bm_words = search_bitmap_words(std::max(1, c.map.n));
 
     // Candidates: visited placement (1 shared-memory bitmap, 2 stamped
-    // records, 3 global bitmap, 4 global bitmap that a search left alone in
-    // its block moves into the block's shared memory) and block size.  The
+    // records, 3 global bitmap, 4 global bitmap that a search at a batch's
+    // tail moves into its block's shared memory) and block size.  The
     // score is the number of resident slots weighted by how close the claim
     // check is: on chip x4, L2 x3, DRAM x2 (the record check misses L2 in
     // every round); placement 4 wins a tie with placement 3 (a frame's tail

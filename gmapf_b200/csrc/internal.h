@@ -67,7 +67,7 @@ struct SearchParams {
     unsigned* gbm;           // visited mode 3: bm_words 32-bit words per slot, global
     int* work_ctr;
     int max_rounds;
-    int promote_rounds;      // visited placement 4: rounds before a search left alone in its block moves its bitmap
+    int promote_rounds;      // visited placement 4: rounds before a search may move its bitmap into shared memory
     // outputs
     int* paths;              // row-major, path_stride ints per row
     long long path_stride;

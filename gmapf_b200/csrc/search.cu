@@ -303,8 +303,8 @@ __device__ __forceinline__ void walk_path(const Rec* rec, int n_nodes, int* out,
 }
 
 // VM: visited placement (1 shared-memory bitmap, 2 stamped records, 3 global
-// bitmap, 4 global bitmap that a search left alone in its block moves into
-// the block's shared memory).  In modes 1, 3 and 4 a bit set by one thread is
+// bitmap, 4 global bitmap that a search still running at a batch's tail
+// moves into the shared memory of its block's finished warps).  In modes 1, 3 and 4 a bit set by one thread is
 // seen by the others after the next __syncwarp (bar.warp.sync orders memory
 // among its threads).
 //

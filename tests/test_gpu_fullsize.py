@@ -2,7 +2,7 @@
 101,698 triangles), 16,384 searches in one batch, 32 threads per agent and
 queue capacity 16 (the shape the autotuner picks for this map), visited
 bitmap in global memory (placement 3) or in global memory and then, for a
-search left alone in its block, in shared memory (placement 4, the default
+search still running at the batch's tail, in shared memory (placement 4, the default
 pick).  Checked through properties that do not depend on
 size: two runs agree bit for bit, a sample agrees with the oracle exactly,
 paths are connected chains of neighbours that end at their targets, and no
@@ -37,7 +37,7 @@ def run(g, s, t):
 
 @pytest.mark.parametrize("vm", [3, 4])
 def test_full_frame_batch(oracle_mod, vm):
-    # placement 4 at its default: searches alone in their blocks move after 512 rounds
+    # placement 4 at its default: searches may move from their 512th round on
     scn = S.cfg3(cells=160)
     g = map_world(scn, T=T, Cap=CAP, visited_mode=vm, promote_rounds=0)
     assert g.node_count > 100_000
