@@ -61,6 +61,7 @@
 
 #include "internal.h"
 #include "records.cuh"
+#include "region_plan.cuh"
 
 namespace gmapf_b200 {
 
@@ -171,44 +172,9 @@ __host__ __device__ __forceinline__ size_t search_frontier_words(int T) {
 }
 
 
-// Placement 4: words after the last warp's share so that all but one share
-// and the pad hold one bitmap (a multiple of 4 words).
-__host__ __device__ __forceinline__ size_t search_pad_words(int bm_words, int warps, int per_warp) {
-    const long long rest = (long long)bm_words - (long long)(warps - 1) * per_warp;
-    return rest > 0 ? (size_t)((rest + 3) & ~3ll) : 0;
-}
-
 // Record word 0 in the bitmap placements: the nearest proper ancestor whose
 // depth (G) is a multiple of kJumpDepth, -1 at a search's root.
 constexpr int kJumpDepth = 256;
-
-// Placement 4: where a search of warp `me` can put its bitmap (bm words) in
-// its block's shared memory, given the warps that have left (`left`, whose
-// shares are free for good).  Shares are `share` words each, `pad` words
-// follow the last one.  The bitmap takes a run of free shares (this warp's
-// own share may be in it), the last run of the block also using the pad;
-// when this warp's share is in the run, its queues move to a free share
-// outside it.  Returns first | home << 8, or -1 when there is no room.
-__device__ __noinline__ int region_plan(unsigned left, int me, int wpb, int share, int bm, int pad) {
-    if (pad >= bm) return wpb | (me << 8);  // the pad alone (one-warp blocks)
-    const unsigned usable = left | (1u << me);
-    for (int first = wpb - 1; first >= 0; first--) {
-        // the run [first, last] with the smallest last that holds the bitmap
-        long long room = 0;
-        int last = first;
-        for (; last < wpb; last++) {
-            if (!((usable >> last) & 1u)) break;
-            room += share + (last == wpb - 1 ? pad : 0);
-            if (room >= bm) break;
-        }
-        if (last >= wpb || room < bm || !((usable >> last) & 1u)) continue;
-        const unsigned run = (last - first >= 31 ? 0xffffffffu : ((2u << (last - first)) - 1u)) << first;
-        if (!((run >> me) & 1u)) return first | (me << 8);
-        const unsigned outside = left & ~run;  // another free share for this warp's queues
-        if (outside) return first | ((__ffs(outside) - 1) << 8);
-    }
-    return -1;
-}
 
 // Path output: depth d of the start side at out[d - 1] (d >= 1), depth d of
 // the target side at out[gS + gT - d] (d >= 0).
