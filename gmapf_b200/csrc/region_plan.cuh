@@ -14,6 +14,14 @@ __host__ __device__ __forceinline__ size_t search_pad_words(int bm_words, int wa
     return rest > 0 ? (size_t)((rest + 3) & ~3ll) : 0;
 }
 
+// The fewest shares (with the pad after the last) that hold the bitmap: a
+// search checks this cheap count in its round loop and works out a plan only
+// when at least that many shares are free; no plan needs fewer.
+__host__ __device__ __forceinline__ int region_shares_needed(int bm_words, int wpb, int share) {
+    const int rest = bm_words - (int)search_pad_words(bm_words, wpb, share);
+    return rest > 0 ? (rest + share - 1) / share : 0;
+}
+
 __host__ __device__ __forceinline__ int lowest_set_bit(unsigned x) {  // 1-based, 0 for none
 #ifdef __CUDA_ARCH__
     return __ffs(x);

@@ -697,12 +697,9 @@ __global__ void __launch_bounds__(256, 3) k_search(SearchParams p, int persisten
                 if ((int)rounds == next_check) {  // warp-uniform
                     next_check += 256;
                     int room = 0;
-                    if (lane == 0) {
-                        const int share = (int)(qblk + fblk);
-                        const int rest = bm_words - (int)search_pad_words(bm_words, wpb, share);
-                        const int need = rest > 0 ? (rest + share - 1) / share : 0;
-                        room = __popc(*reinterpret_cast<volatile unsigned*>(&block_left) | (1u << wib)) >= need;
-                    }
+                    if (lane == 0)
+                        room = __popc(*reinterpret_cast<volatile unsigned*>(&block_left) | (1u << wib)) >=
+                               region_shares_needed(bm_words, wpb, (int)(qblk + fblk));
                     if (__shfl_sync(kFull, room, 0)) return false;
                 }
             }

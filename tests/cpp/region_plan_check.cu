@@ -3,13 +3,15 @@
 // left and every warp still running, a plan must keep the bitmap inside the
 // block's shared memory, cover only free shares (or the warp's own), and put
 // the warp's queues in its own share or in a free share outside the bitmap;
-// a warp whose block-mates have all left must always get a plan.  Built with
+// a warp whose block-mates have all left must always get a plan, and the
+// round loop's count of free shares must never turn away a plan.  Built with
 // nvcc as host code and run by tests/test_region_plan.py.
 #include <cstdio>
 
 #include "region_plan.cuh"
 
 using gmapf_b200::region_plan;
+using gmapf_b200::region_shares_needed;
 using gmapf_b200::search_pad_words;
 
 int main() {
@@ -36,6 +38,12 @@ int main() {
                             continue;
                         }
                         plans++;
+                        // the round loop's cheap count must let every plan through
+                        if (__builtin_popcount(left | (1u << me)) < region_shares_needed(bm, wpb, share)) {
+                            std::printf("FAIL count vetoes a plan: wpb=%d share=%d bm=%d left=%x me=%d\n", wpb,
+                                        share, bm, left, me);
+                            return 1;
+                        }
                         const int first = r & 0xff, home = r >> 8;
                         const long long start = (long long)first * share, end = start + bm;
                         bool ok = first >= 0 && first <= wpb && home >= 0 && home < wpb && end <= total;
